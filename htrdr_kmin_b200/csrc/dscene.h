@@ -1,0 +1,81 @@
+/* Device-side views of a scene and of a request (plain structs passed by
+ * value to the kernels).  Shared by the host code that fills them and the
+ * kernels that read them. */
+#ifndef HTRDR_DSCENE_H
+#define HTRDR_DSCENE_H
+
+#include <stdint.h>
+
+#define HG_LEAF 0xFFFFFFFFu
+#define HG_MAX_DIST 1e9f          /* no collision beyond (..._sw.c:118-123) */
+#define HG_TMIN_ZERO 746.0        /* exp(-Tmin) == 0.0 in FP64 from here on */
+#define HG_MAX_STEPS (1u << 20)   /* voxel steps per trace before giving up */
+#define HG_MAX_BOUNCES (1u << 16) /* scattering events per realisation before giving up */
+#define HG_MAX_NULL (1u << 22)    /* tentative collisions per voxel before giving up */
+
+enum { HG_KA = 0, HG_KS = 1, HG_KEXT = 2 };
+enum { HG_XWAVE_SW = 0, HG_XWAVE_LW = 1, HG_IMAGE_CIE = 2, HG_FLUX_SW = 3, HG_FLUX_LW = 4 };
+
+struct DScene {
+  /* gas column */
+  uint32_t nlayers;
+  const float* layer_z;   /* [nlayers+1] */
+  const float* layer_T;   /* [nlayers] */
+  float ztop;
+  const float2* gas;      /* [nq][nlayers] {ka, ks} */
+  /* spectral */
+  uint32_t nbands;
+  const double* band_lo;  /* [nbands] */
+  const double* band_hi;  /* [nbands] */
+  const uint32_t* quad_off; /* [nbands+1] */
+  const double* quad_cum; /* [nq] */
+  const float4* optics;   /* [nbands] {sigma_a, sigma_s, sigma_ext, g} */
+  /* cloud */
+  int32_t has_cloud, repeat;
+  uint32_t def[3];
+  float lower[3], upper[3], cell[3], inv_cell[3];
+  const float* lwc;       /* [nz][ny][nx] */
+  const int2* cell_layers;/* [nz] first/last gas layer overlapping the z-cell */
+  uint32_t depth;
+  const uint4* nodes;     /* node pool */
+  const uint64_t* tree_base; /* [nq*3]: first node of the octree (q, prop) */
+  /* ground */
+  int32_t has_ground, ground_brdf;
+  float ground_refl, ground_T;
+  /* sun */
+  float sun_dir[3], sun_b1[3], sun_b2[3];
+  double sun_dir_d[3];
+  double sun_cos_half, sun_solid_angle, sun_T;
+};
+
+struct DRequest {
+  int32_t mode;
+  uint32_t width, height, spp, nreal_pp; /* nreal_pp = spp (x3 for CIE) */
+  uint32_t seed;
+  uint64_t acc_base;     /* first channel accumulator of this request */
+  uint64_t tacc_base;    /* first time accumulator of this request */
+  double pix_sz[2];
+  double wlen_range[2];  /* nm */
+  /* wavelength sampler */
+  uint32_t ncdf;         /* CDF length (0: continuous/monochromatic) */
+  double band_len;
+  const double* cdf;     /* Planck: [ncdf]; CIE: [3][ncdf] */
+  const double* pdf;     /* Planck: [ncdf] */
+  const double* fbound;  /* CIE: [3][ncdf][2] fit values at each band's bounds */
+  double rcp_integral[3];
+  double ref_T;
+  /* camera */
+  int32_t camera_type;
+  double cam_pos[3], cam_f[3], cam_r[3], cam_u[3];
+  double tan_half, aspect, lens_radius, focal_dst, ortho_h;
+  /* flux rectangle */
+  double rect_pos[3], rect_ax[3], rect_ay[3], rect_n[3];
+};
+
+/* Per-pixel FP64 accumulators (one per channel) and per-pixel time */
+struct DAccum {
+  double s, s2;
+  unsigned long long n, pad;
+};
+
+#endif

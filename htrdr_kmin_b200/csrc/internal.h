@@ -1,0 +1,110 @@
+/* Internal host-side declarations of the CUDA library. */
+#ifndef HTRDR_INTERNAL_H
+#define HTRDR_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/htrdr_gpu.h"
+#include "dscene.h"
+
+namespace hg {
+
+void set_error(const std::string& msg);
+bool cuda_ok(cudaError_t e, const char* what);
+
+/* Device allocation owned by a scene or a request cache */
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf();
+  bool alloc(size_t n);
+  bool upload(const void* src, size_t n);
+};
+
+/* Wavelength sampler tables of a request, on the device */
+struct Sampler {
+  int mode_cie = 0;
+  uint32_t ncdf = 0;
+  double band_len = 0;
+  double rcp_integral[3] = {0, 0, 0};
+  DevBuf cdf, pdf, fbound;
+  std::vector<double> host_cdf; /* for the host-side checks */
+};
+
+}  // namespace hg
+
+struct htrdr_gpu_scene {
+  int device = 0;
+  DScene d{};
+  uint32_t nbands = 0, nq = 0, nlayers = 0, props_mask = 0, depth = 0;
+  std::vector<double> band_lo, band_hi;
+  std::vector<uint32_t> nquads, quad_off;
+  std::vector<uint64_t> tree_base, tree_count;
+  std::vector<std::unique_ptr<hg::DevBuf>> bufs;
+  size_t bytes = 0;
+  /* Wavelength samplers keyed by (cie, range0, range1, Tref) */
+  std::map<std::tuple<int, double, double, double>, std::unique_ptr<hg::Sampler>> samplers;
+  std::mutex mtx;
+  cudaStream_t stream = nullptr;
+};
+
+namespace hg {
+
+/* Host spectral routines (same definitions as the reference's
+ * src/core/htrdr_spectral.h and samplers) */
+double wiebelt(double v);
+double blackbody_fraction(double l0, double l1, double T);
+double fit_bar_1931(int channel, double lambda);
+double cie_trapezoid(double lo, double hi, int channel);
+
+/* Sampler of a request (built on first use and cached in the scene) */
+Sampler* scene_sampler(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, htrdr_gpu_res_T* res);
+/* Fill the device view of a request */
+htrdr_gpu_res_T make_drequest(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, DRequest* out);
+uint32_t pixel_size(int mode);
+
+/* Octree build on the host, bit-exact definition shared with the oracle.
+ * Writes nodes[4*i..] = {kmin bits, kmax bits, child, 0}. */
+void build_octree(const DScene& hs, const float* lwc, const float* sig3, const float* gas_ka,
+                  const float* gas_ks, const int* cl_lo, const int* cl_hi, uint32_t q, int prop,
+                  uint32_t depth, uint32_t level_force, double tau, double cmax,
+                  std::vector<uint32_t>& nodes);
+
+/* Kernel launchers (kernels.cu) */
+struct LaunchOut {
+  unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
+  float kernel_ms = 0;
+};
+cudaError_t launch_plain(const DScene& S, const DRequest& R, DAccum* acc, DAccum* tacc,
+                         uint64_t pix_begin, uint32_t npix, double* weights, void* counters,
+                         cudaStream_t st);
+cudaError_t launch_finalize(const DRequest& R, const DAccum* acc, const DAccum* tacc,
+                            void* out, size_t pitch, cudaStream_t st);
+cudaError_t launch_radiance(const DScene& S, int lw, size_t n, const double* pos,
+                            const double* dir, const double* wlen, const uint32_t* band,
+                            const uint32_t* iquad, int mask, uint32_t seed, double* out,
+                            cudaStream_t st);
+cudaError_t launch_find_band(const DScene& S, size_t n, const double* wlen, uint32_t* out,
+                             cudaStream_t st);
+cudaError_t launch_sample_quad(const DScene& S, size_t n, const double* r, const uint32_t* band,
+                               uint32_t* out, cudaStream_t st);
+cudaError_t launch_locate_leaf(const DScene& S, uint32_t q, int prop, size_t n,
+                               const uint32_t* cells, uint32_t* node, uint32_t* level,
+                               cudaStream_t st);
+cudaError_t launch_sample_wavelength(const DRequest& R, int channel, size_t n, const double* r0,
+                                     const double* r1, uint32_t* cb, double* wlen, double* pdf,
+                                     cudaStream_t st);
+
+}  // namespace hg
+
+#endif

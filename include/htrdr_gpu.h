@@ -1,0 +1,224 @@
+/* htrdr_gpu.h -- C ABI of the B200 (sm_100a) atmosphere path tracer.
+ *
+ * A drop-in for the hot path of htrdr-atmosphere (AnthonyArfaux/htrdr_kmin):
+ * the htrdr_draw_map driver with the atmosphere per-pixel / per-probe
+ * realisation callbacks, the shortwave and longwave radiance routines and
+ * the per-(band, quadrature point) kmin/kmax majorant octrees of htsky.
+ * Plain C types only; every buffer argument is a host pointer unless the
+ * function name ends in _device.  Return codes follow rsys res_T.
+ *
+ * No CPU fallback: every entry point that computes runs CUDA kernels and
+ * returns HTRDR_GPU_RES_BAD_OP when no usable device is present. */
+#ifndef HTRDR_GPU_H
+#define HTRDR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+  #define HTRDR_GPU_API __attribute__((visibility("default")))
+#else
+  #define HTRDR_GPU_API
+#endif
+
+/* rsys res_T values (RES_OK, RES_BAD_ARG, RES_MEM_ERR, RES_IO_ERR,
+ * RES_UNKNOWN_ERR, RES_BAD_OP) */
+typedef int htrdr_gpu_res_T;
+#define HTRDR_GPU_RES_OK 0
+#define HTRDR_GPU_RES_BAD_ARG 1
+#define HTRDR_GPU_RES_MEM_ERR 2
+#define HTRDR_GPU_RES_IO_ERR 3
+#define HTRDR_GPU_RES_UNKNOWN_ERR 4
+#define HTRDR_GPU_RES_BAD_OP 5
+
+/* Output/spectral mode = the atmosphere draw_pixel callback that
+ * atmosphere_draw_map selects (src/atmosphere/htrdr_atmosphere_draw_map.c:438-475) */
+enum htrdr_gpu_mode {
+  HTRDR_GPU_XWAVE_SW = 0,  /* draw_pixel_xwave, shortwave  (:324-436) */
+  HTRDR_GPU_XWAVE_LW = 1,  /* draw_pixel_xwave, longwave   (:324-436) */
+  HTRDR_GPU_IMAGE_CIE = 2, /* draw_pixel_image, CIE XYZ    (:109-207) */
+  HTRDR_GPU_FLUX_SW = 3,   /* draw_pixel_flux, shortwave   (:209-322) */
+  HTRDR_GPU_FLUX_LW = 4    /* draw_pixel_flux, longwave    (:209-322) */
+};
+
+/* Radiance components (enum atmosphere_radiance_cpnt_flag,
+ * src/atmosphere/htrdr_atmosphere_c.h:38-44) */
+#define HTRDR_GPU_RADIANCE_DIRECT 1
+#define HTRDR_GPU_RADIANCE_DIFFUSE 2
+#define HTRDR_GPU_RADIANCE_ALL 3
+
+/* Medium properties (enum htsky_property) */
+#define HTRDR_GPU_KA 0
+#define HTRDR_GPU_KS 1
+#define HTRDR_GPU_KEXT 2
+
+/* Medium, ground and sun: what htsky_create, htrdr_atmosphere_ground_create
+ * and htrdr_atmosphere_sun_create set up in htrdr_atmosphere_create
+ * (src/atmosphere/htrdr_atmosphere.c:353-382). */
+struct htrdr_gpu_scene_desc {
+  uint32_t nlayers;
+  const double* layer_z;        /* [nlayers+1] layer bounds in m, ascending, from 0 */
+  const float* layer_T;         /* [nlayers] temperature in K */
+  uint32_t nbands;
+  const double* band_lo;        /* [nbands] nm */
+  const double* band_hi;        /* [nbands] nm */
+  const uint32_t* nquads;       /* [nbands] quadrature points per band */
+  const double* quad_w;         /* [sum nquads] quadrature weights (sum 1 per band) */
+  const float* gas_ka;          /* [sum nquads][nlayers] 1/m */
+  const float* gas_ks;          /* [sum nquads][nlayers] 1/m */
+  uint32_t cloud_def[3];        /* nx, ny, nz; all 0 = clear sky */
+  double cloud_lower[3];        /* m */
+  double cloud_cell[3];         /* m */
+  const float* cloud_lwc;       /* [nz][ny][nx] kg/m^3 */
+  const float* cloud_sigma_ext; /* [nbands] m^2/kg */
+  const float* cloud_ssa;       /* [nbands] */
+  const float* cloud_g;         /* [nbands] Henyey-Greenstein asymmetry */
+  int32_t repeat_clouds;        /* -r */
+  double optical_thickness;     /* -T: majorant merge threshold */
+  uint32_t grid_max_definition[3]; /* -V: 0 = cloud definition */
+  int32_t has_ground;
+  int32_t ground_brdf;          /* 0 Lambertian, 1 specular */
+  double ground_reflectivity;
+  double ground_temperature;    /* K */
+  double sun_azimuth, sun_elevation; /* -D, degrees */
+  uint32_t props_mask;          /* bit p: build the majorants of property p */
+};
+
+/* One run of the atmosphere command: sensor, spectral domain, output type
+ * and spp (htrdr_atmosphere_args). */
+struct htrdr_gpu_request {
+  int32_t mode;                 /* enum htrdr_gpu_mode */
+  uint32_t width, height, spp;
+  double wlen_range[2];         /* nm */
+  double ref_temperature;       /* K */
+  int32_t camera_type;          /* 0 perspective, 1 orthographic */
+  double cam_pos[3], cam_tgt[3], cam_up[3];
+  double fov_deg, lens_radius, focal_dst, ortho_height;
+  double rect_pos[3], rect_tgt[3], rect_up[3], rect_size[2];
+  uint32_t seed;
+};
+
+/* struct htrdr_buffer_layout (src/core/htrdr_buffer.h:44-50) */
+struct htrdr_gpu_buffer_layout {
+  size_t width, height, pitch, elmt_size, alignment;
+};
+
+/* Device counters of one launch */
+struct htrdr_gpu_stats {
+  uint64_t realisations; /* completed realisations */
+  uint64_t segments;     /* voxels (octree leaves + gas layers) visited */
+  uint64_t nodes;        /* majorant nodes fetched */
+  uint64_t collisions;   /* tentative collisions */
+  uint64_t failures;     /* traces stopped by the step guard */
+  double kernel_ms;      /* CUDA-event time of the transport kernel(s) */
+  double total_ms;       /* whole call, device side */
+};
+
+struct htrdr_gpu_scene;
+struct htrdr_gpu_server;
+
+/* ---- scene (replaces htsky_create: src/atmosphere/htrdr_atmosphere.c:366-382) ---- */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_scene_create(int device, const struct htrdr_gpu_scene_desc* desc,
+                       struct htrdr_gpu_scene** scene);
+HTRDR_GPU_API void htrdr_gpu_scene_release(struct htrdr_gpu_scene* scene);
+/* Device bytes held by the scene (medium + octrees) */
+HTRDR_GPU_API size_t htrdr_gpu_scene_device_bytes(const struct htrdr_gpu_scene* scene);
+/* Copy one majorant octree to the host as 16-byte {kmin, kmax, child, 0}
+ * nodes (what htsky_dump_cloud_vtk writes, src/atmosphere/htrdr_atmosphere.c:196-224).
+ * With nodes == NULL only *count is set. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_scene_get_tree(const struct htrdr_gpu_scene* scene, uint32_t iband, uint32_t iquad,
+                         int prop, void* nodes, size_t capacity, size_t* count);
+HTRDR_GPU_API uint32_t htrdr_gpu_scene_tree_depth(const struct htrdr_gpu_scene* scene);
+
+/* ---- plain drop-in driver: htrdr_draw_map(htrdr, args, buf) with the atmosphere
+ * callbacks (src/core/htrdr_draw_map.h:89-93, src/atmosphere/htrdr_atmosphere_draw_map.c:592-641).
+ * Fills `buffer' (host memory, `layout') with atmosphere_pixel_{xwave,flux,image}
+ * structs (src/atmosphere/htrdr_atmosphere_c.h:46-76). ---- */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_map(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                   const struct htrdr_gpu_buffer_layout* layout, void* buffer,
+                   struct htrdr_gpu_stats* stats);
+/* Same, output written to device memory (no host copy). */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_map_device(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                          const struct htrdr_gpu_buffer_layout* layout, void* device_buffer,
+                          struct htrdr_gpu_stats* stats);
+
+/* ---- radiance routines, batched: atmosphere_compute_radiance_sw / _lw
+ * (src/atmosphere/htrdr_atmosphere_c.h:140-163).  Ray i uses the random
+ * stream keyed by (i, seed).  out[i] in W/m^2/sr/m. ---- */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_radiance_sw(struct htrdr_gpu_scene* scene, size_t n, const double* pos,
+                      const double* dir, const double* wlen, const uint32_t* iband,
+                      const uint32_t* iquad, int cpnt_mask, uint32_t seed, double* out);
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_radiance_lw(struct htrdr_gpu_scene* scene, size_t n, const double* pos,
+                      const double* dir, const double* wlen, const uint32_t* iband,
+                      const uint32_t* iquad, uint32_t seed, double* out);
+
+/* Per-realisation weights of pixels [pix_begin, pix_end) of a request
+ * (NaN for rejected samples): one-to-one comparison with a CPU restatement. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_realisation_weights(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                              size_t pix_begin, size_t pix_end, double* weights);
+
+/* ---- integer work, exposed for bit-exact checks ---- */
+/* htsky_find_spectral_band (called at src/atmosphere/htrdr_atmosphere_draw_map.c:176) */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_find_band(struct htrdr_gpu_scene* scene, size_t n, const double* wlen, uint32_t* out);
+/* htsky_spectral_band_sample_quadrature (draw_map.c:177) */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_sample_quad(struct htrdr_gpu_scene* scene, size_t n, const double* r,
+                      const uint32_t* iband, uint32_t* out);
+/* Octree point location: leaf node index and level of integer cells [n][3] */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_locate_leaf(struct htrdr_gpu_scene* scene, uint32_t iband, uint32_t iquad, int prop,
+                      size_t n, const uint32_t* cells, uint32_t* node, uint32_t* level);
+/* Wavelength sampling of a request (htrdr_ran_wlen_planck_sample /
+ * htrdr_ran_wlen_cie_xyz_sample_{X,Y,Z}): CDF band index, wavelength, pdf. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_sample_wavelength(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                            int channel, size_t n, const double* r0, const double* r1,
+                            uint32_t* cdf_band, double* wlen, double* pdf);
+
+/* ---- batched engine: many requests in one persistent kernel ---- */
+struct htrdr_gpu_batch_item {
+  struct htrdr_gpu_scene* scene;
+  struct htrdr_gpu_request req;
+  struct htrdr_gpu_buffer_layout layout;
+  void* buffer; /* host */
+};
+struct htrdr_gpu_tuning {
+  uint32_t block_size;    /* threads per block of the persistent kernel */
+  uint32_t queue_chunk;   /* realisations taken from the work queue at once */
+  uint32_t regroup_period;/* transport steps between two live-path regroupings */
+  uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
+};
+/* Renders every item (each one htrdr_draw_map call of the reference) in one
+ * persistent kernel; item buffers are host memory. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_maps_batched(struct htrdr_gpu_batch_item* items, size_t n,
+                            const struct htrdr_gpu_tuning* tuning, struct htrdr_gpu_stats* stats);
+/* Same, item buffers are device memory (no host copy). */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_maps_batched_device(struct htrdr_gpu_batch_item* items, size_t n,
+                                   const struct htrdr_gpu_tuning* tuning,
+                                   struct htrdr_gpu_stats* stats);
+HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
+
+/* ---- library info ---- */
+HTRDR_GPU_API const char* htrdr_gpu_version(void);
+HTRDR_GPU_API int htrdr_gpu_device_count(void);
+HTRDR_GPU_API const char* htrdr_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HTRDR_GPU_H */

@@ -188,6 +188,10 @@ int ora_draw_map(const struct ora_scene* scn, const struct ora_request* req, voi
                  size_t pitch, size_t pix_begin, size_t pix_end, int nthreads,
                  struct ora_counters* cnt);
 
+int ora_sample_wavelength(const struct ora_scene* scn, const struct ora_request* req, int channel,
+                          size_t n, const double* r0, const double* r1, uint32_t* cdf_band,
+                          double* wlen, double* pdf);
+
 /* Per-realisation weights for pixels [pix_begin, pix_end) (realisation-major
  * inside a pixel): the matched-stream comparison with the GPU. */
 int ora_realisation_weights(const struct ora_scene* scn, const struct ora_request* req,

@@ -386,6 +386,29 @@ ora_draw_map(const struct ora_scene* scn, const struct ora_request* req, void* b
   return ORA_RES_OK;
 }
 
+/* Wavelength sampling of a request (CDF band, wavelength in nm, pdf in nm^-1) */
+int
+ora_sample_wavelength(const struct ora_scene* scn, const struct ora_request* req, int channel,
+                      size_t n, const double* r0, const double* r1, uint32_t* cdf_band,
+                      double* wlen, double* pdf)
+{
+  struct drv dv;
+  size_t i;
+  int res = drv_init(&dv, scn, req);
+  if(res != ORA_RES_OK) return res;
+  for(i = 0; i < n; ++i) {
+    if(req->mode == ORA_IMAGE_CIE) {
+      cdf_band[i] = (uint32_t)ora_cie_ran_band(&dv.cie, channel, r0[i]);
+      wlen[i] = ora_cie_ran_sample(&dv.cie, channel, r0[i], r1[i], &pdf[i]);
+    } else {
+      cdf_band[i] = dv.planck.nbands ? (uint32_t)ora_planck_ran_band(&dv.planck, r0[i]) : 0;
+      wlen[i] = ora_planck_ran_sample(&dv.planck, r0[i], r1[i], &pdf[i]);
+    }
+  }
+  drv_release(&dv);
+  return ORA_RES_OK;
+}
+
 int
 ora_realisation_weights(const struct ora_scene* scn, const struct ora_request* req,
                         size_t pix_begin, size_t pix_end, double* weights, int nthreads)

@@ -228,6 +228,9 @@ transmissivity_hit_filter(const struct ora_seg* seg, const double o[3], const do
   struct sctx* ctx = c;
   const double kmin = seg->kmin, kmax = seg->kmax;
   ctx->Tmin += (seg->distance[1] - seg->distance[0]) * kmin;
+  /* From here on exp(-Tmin) is exactly 0.0 in FP64: the transmissivity is
+   * zero whatever else happens, so stop like a real collision would. */
+  if(ctx->Tmin >= 746.0) return 0;
   ctx->traversal_dst = seg->distance[0];
   for(;;) {
     const double Tdif = (seg->distance[1] - ctx->traversal_dst) * (kmax - kmin);

@@ -23,9 +23,14 @@ DIRECT, DIFFUSE, ALL = 1, 2, 3
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (gcc + OpenMP)."""
-    if force or not os.path.exists(_LIB_PATH):
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile the oracle with its Makefile (gcc + OpenMP); make skips it when
+    the library is up to date.  Without make (or a compiler) an existing build
+    is used as is."""
+    try:
+        subprocess.run(["make", "-s", "-C", _HERE] + (["-B"] if force else []), check=True)
+    except (OSError, subprocess.CalledProcessError):
+        if not os.path.exists(_LIB_PATH):
+            raise
     return _LIB_PATH
 
 
@@ -114,6 +119,10 @@ def lib() -> C.CDLL:
                                          C.POINTER(C.c_double), C.POINTER(C.c_uint32),
                                          C.POINTER(C.c_uint32), C.c_int, C.c_uint32,
                                          C.POINTER(C.c_double), C.c_int]
+        L.ora_sample_wavelength.argtypes = [C.c_void_p, C.POINTER(RequestDesc), C.c_int,
+                                            C.c_size_t, C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]
         for name in ("ora_wiebelt",):
             getattr(L, name).argtypes = [C.c_double]
             getattr(L, name).restype = C.c_double
@@ -233,6 +242,21 @@ class OracleScene:
         if res != 0:
             raise RuntimeError(f"ora_draw_map failed: {res}")
         return buf, {"nseg": cnt.nseg, "nnode": cnt.nnode, "ntc": cnt.ntc, "nreal": cnt.nreal}
+
+    def sample_wavelength(self, req, channel: int, r0, r1):
+        r0 = np.ascontiguousarray(r0, np.float64)
+        r1 = np.ascontiguousarray(r1, np.float64)
+        n = len(r0)
+        cb = np.zeros(n, np.uint32)
+        wl = np.zeros(n, np.float64)
+        pdf = np.zeros(n, np.float64)
+        rd = request_desc(req)
+        res = lib().ora_sample_wavelength(self.handle, C.byref(rd), channel, n, _p(r0, C.c_double),
+                                          _p(r1, C.c_double), _p(cb, C.c_uint32),
+                                          _p(wl, C.c_double), _p(pdf, C.c_double))
+        if res != 0:
+            raise RuntimeError(res)
+        return cb, wl, pdf
 
     def realisation_weights(self, req, pix_begin: int, pix_end: int, nthreads: int = 0):
         nr = req.realisations_per_pixel

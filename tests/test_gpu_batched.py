@@ -1,0 +1,95 @@
+"""Batched persistent kernel vs the plain one-thread-per-realisation kernel.
+
+Both run the same per-realisation state machine on the same Philox stream,
+so every pixel sums the same weights; only the FP64 summation order differs
+(tolerance 1e-9 relative).  A request gives the same result alone and in a
+mix of other requests, scenes and modes."""
+import numpy as np
+import pytest
+
+from htrdr_kmin_b200 import scene as S
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-9
+
+
+def _cmp(a, b, mode):
+    if mode in (S.MODE_FLUX_SW, S.MODE_FLUX_LW):
+        np.testing.assert_array_equal(a["n"], b["n"])
+        np.testing.assert_allclose(a["sum"], b["sum"], rtol=RTOL, atol=0)
+        np.testing.assert_allclose(a["sum2"], b["sum2"], rtol=RTOL, atol=0)
+    elif mode == S.MODE_IMAGE_CIE:
+        for c in ("X", "Y", "Z"):
+            np.testing.assert_allclose(a[c], b[c], rtol=RTOL, atol=0)
+            np.testing.assert_allclose(a[c + "_se"], b[c + "_se"], rtol=1e-6, atol=1e-300)
+    else:
+        np.testing.assert_allclose(a["L"], b["L"], rtol=RTOL, atol=0)
+        np.testing.assert_allclose(a["L_se"], b["L_se"], rtol=1e-6, atol=1e-300)
+        np.testing.assert_allclose(a["Tb"], b["Tb"], rtol=1e-6, atol=0)
+    np.testing.assert_array_equal(a["t_n"], b["t_n"])
+
+
+def _mix(gpu_lib):
+    s1, r1 = S.config_c1(scale=20 / 64, spp=16)
+    s2, r2 = S.config_c2(scale=24 / 128, spp=24, cloud_def=(16, 16, 8))
+    s3, r3 = S.config_c3(scale=13 / 512, spp=6, cloud_def=(32, 32, 8), nbands=6, nquad=3)
+    g1, g2, g3 = gpu_lib.GpuScene(s1), gpu_lib.GpuScene(s2, 0b100), gpu_lib.GpuScene(s3)
+    r4 = S.Request(**{**r2.__dict__, "mode": S.MODE_XWAVE_LW, "width": 9, "height": 7,
+                      "cam_pos": (800, 800, 10), "cam_tgt": (900, 900, 1500), "cam_up": (0, 1, 0),
+                      "seed": 77})
+    return [(g1, r1), (g2, r2), (g3, r3), (g2, r4)]
+
+
+def test_batched_equals_plain(gpu_lib):
+    items = _mix(gpu_lib)
+    bufs, st = gpu_lib.draw_maps_batched(items)
+    assert st["failures"] == 0
+    for (gs, req), b in zip(items, bufs):
+        p, _ = gs.draw_map(req)
+        _cmp(b, p, req.mode)
+
+
+def test_alone_equals_in_mix(gpu_lib):
+    items = _mix(gpu_lib)
+    mixed, _ = gpu_lib.draw_maps_batched(items)
+    for i, it in enumerate(items):
+        alone, _ = gpu_lib.draw_maps_batched([it])
+        _cmp(alone[0], mixed[i], it[1].mode)
+
+
+@pytest.mark.parametrize("chunk,bs", [(1, 32), (3, 64), (16, 256)])
+def test_tuning_does_not_change_results(gpu_lib, chunk, bs):
+    items = _mix(gpu_lib)[:2]
+    ref, _ = gpu_lib.draw_maps_batched(items)
+    t = gpu_lib.default_tuning()
+    t.queue_chunk, t.block_size = chunk, bs
+    out, _ = gpu_lib.draw_maps_batched(items, t)
+    for (gs, req), a, b in zip(items, out, ref):
+        _cmp(a, b, req.mode)
+
+
+def test_edge_cases(gpu_lib):
+    sc, rq = S.config_c1(scale=1 / 64, spp=1)   # 1x1 image, one realisation
+    gs = gpu_lib.GpuScene(sc)
+    buf, st = gs.draw_map(rq)
+    assert buf.shape == (1, 1) and buf["t_n"][0, 0] == 1
+    rq2 = S.Request(**{**rq.__dict__, "width": 13, "height": 3, "spp": 2})  # ragged tiles
+    buf, st = gs.draw_map(rq2)
+    assert np.all(buf["t_n"] == 2)
+    bad = S.Request(**{**rq.__dict__, "spp": 0})
+    with pytest.raises(gpu_lib.HtrdrError) as e:
+        gs.draw_map(bad)
+    assert e.value.code == gpu_lib.RES_BAD_ARG
+    # an LW-only scene cannot serve SW requests (missing majorants)
+    s2, r2 = S.config_c2(scale=1 / 64, spp=1, cloud_def=(4, 4, 2))
+    g2 = gpu_lib.GpuScene(s2, 0b100)
+    with pytest.raises(gpu_lib.HtrdrError):
+        g2.draw_map(S.Request(**{**r2.__dict__, "mode": S.MODE_FLUX_SW}))
+    # clear sky and no ground
+    slab = S.homogeneous_slab(k_abs=1e-5, k_sca=1e-5, has_ground=False)
+    gsl = gpu_lib.GpuScene(slab)
+    r3 = S.Request(mode=S.MODE_XWAVE_SW, width=4, height=4, spp=8, wlen_range=(550.0, 550.0),
+                   cam_pos=(0, 0, 500), cam_tgt=(0, 1000, 500), cam_up=(0, 0, 1))
+    buf, st = gsl.draw_map(r3)
+    assert np.all(np.isfinite(buf["L"])) and st["failures"] == 0

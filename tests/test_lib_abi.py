@@ -1,0 +1,59 @@
+"""The C-ABI library loads, exports every function include/htrdr_gpu.h
+declares, and refuses to compute without a GPU (no CPU fallback).  No GPU
+needed."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from htrdr_kmin_b200 import api, build
+from htrdr_kmin_b200 import scene as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "htrdr_gpu.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(htrdr_gpu_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_function():
+    path = build.build()
+    lib = C.CDLL(path)
+    names = header_functions()
+    assert len(names) >= 19
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(api.EXPORTED) <= set(names)
+
+
+def test_version_and_no_device_behaviour():
+    L = api.lib()
+    assert b"sm_100a" in L.htrdr_gpu_version()
+    ndev = api.device_count()
+    if ndev == 0:
+        # no CPU fallback: creating a scene without a device is refused
+        sc, _ = S.config_c1(scale=0.125)
+        with pytest.raises(api.HtrdrError) as e:
+            api.GpuScene(sc)
+        assert e.value.code == api.RES_BAD_OP
+
+
+def test_bad_arguments_are_rejected_before_any_device_work():
+    L = api.lib()
+    h = C.c_void_p()
+    assert L.htrdr_gpu_scene_create(0, None, C.byref(h)) == api.RES_BAD_ARG
+    st = api.Stats()
+    assert L.htrdr_gpu_draw_map(None, None, None, None, C.byref(st)) == api.RES_BAD_ARG
+    assert L.htrdr_gpu_draw_maps_batched(None, 0, None, None) == api.RES_BAD_ARG
+
+
+def test_pixel_layouts_match_reference_structs():
+    # atmosphere_pixel_xwave / _flux / _image (src/atmosphere/htrdr_atmosphere_c.h:46-76)
+    assert api.PIXEL_XWAVE.itemsize == 64
+    assert api.PIXEL_FLUX.itemsize == 64
+    assert api.PIXEL_IMAGE.itemsize == 80
+    assert C.sizeof(api.BufferLayout) == 40
