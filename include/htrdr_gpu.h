@@ -150,6 +150,19 @@ htrdr_gpu_draw_map_device(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_
                           const struct htrdr_gpu_buffer_layout* layout, void* device_buffer,
                           struct htrdr_gpu_stats* stats);
 
+/* Same as htrdr_gpu_draw_map_device without allocating device memory, for
+ * callers that cannot allocate while they render (an application that owns
+ * all of HBM through its own pool, a loop that must not pay for the device
+ * synchronisation of cudaFree).  No counterpart in the reference.  Scratch
+ * (FP64 accumulators, counters, sampler tables) lives in fixed static device
+ * arrays: pixels x (channels + 1) <= 65536 and a wavelength CDF of at most
+ * 131072 entries (29127 bands for CIE), else HTRDR_GPU_RES_BAD_ARG.  The
+ * first call on a device looks the arrays up (make it before any stream
+ * capture); calls whose GPU work overlaps race on the shared arrays. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_map_noalloc(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                           const struct htrdr_gpu_buffer_layout* layout, void* device_buffer);
+
 /* ---- radiance routines, batched: atmosphere_compute_radiance_sw / _lw
  * (src/atmosphere/htrdr_atmosphere_c.h:140-163).  Ray i uses the random
  * stream keyed by (i, seed).  out[i] in W/m^2/sr/m. ---- */
