@@ -1,28 +1,35 @@
 """Benchmark of the B200 atmosphere path tracer (one JSON line on rank 0).
 
-Workload: the longwave flux map -- 128 x 128 ground probes x 256
-realisations, 16 bands x 8 correlated-k points, 50 gas layers with
-per-layer k log-uniform in [1e-6, 1e2] 1/m, 64 x 64 x 32 lognormal cloud
-repeated along X and Y, emissivity-0.95 ground (synthetic, seeded).  A step
-is one htrdr_draw_map of that map.
+Default workload (``--workload lw_flux``): the longwave flux map -- 128 x 128
+ground probes x 256 realisations, 16 bands x 8 correlated-k points, 50 gas
+layers with per-layer k log-uniform in [1e-6, 1e2] 1/m, 64 x 64 x 32
+lognormal cloud repeated along X and Y, emissivity-0.95 ground (synthetic,
+seeded).  A step is one htrdr_draw_map of that map.
 
 * value: Mrealisations/s of the batched persistent kernel, output kept in
   HBM, scene (octrees) resident; device time from CUDA events recorded on the
   library's stream, max over ranks.
 * e2e: the same through the C ABI with a pinned host buffer
   (htrdr_gpu_draw_map: request in, pixel buffer copied back), wall clock.
+* plain_gpu: the one-thread-per-realisation drop-in kernel on the same work.
 * --impl reference: the CPU restatement of the reference path (oracle,
   OpenMP over all host cores) on a bounded sample of the same map.
 
+Other workloads (development and profiling): ``sw_image`` (SW image 64x64 x 32
+spp, one band at 550 nm, 32x32x16 cloud), ``cie_image`` (CIE image 256x256 x
+16 spp x 3 channels, 30 bands x 16 points, 128x128x32 power-law cloud) and
+``mix`` (24 uneven SW/LW image requests on three scenes in one launch, against
+the same requests one at a time on the plain kernel).
+
 Multi-GPU (torchrun): every rank renders the whole map with its own random
-streams (weak scaling) and the per-probe FP64 accumulators are summed on rank
-0 with NCCL.
+streams (weak scaling) and, for flux maps, the per-probe FP64 accumulators are
+summed on rank 0 with NCCL.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
-import math
 import os
 import subprocess
 import sys
@@ -46,6 +53,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="lw_flux", choices=["lw_flux", "sw_image", "cie_image", "mix"])
     p.add_argument("--cpu-sample-s", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -122,53 +130,66 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload():
-    return S.config_c2()
+def workload(name: str):
+    """List of (scene index, request) and the scenes, plus a description."""
+    if name == "lw_flux":
+        sc, rq = S.config_c2()
+        return [sc], [(0, rq)], ("LW flux map 128x128 probes x 256 realisations/probe, 16 bands x 8 "
+                                 "quad, 50 layers, cloud 64x64x32 repeated")
+    if name == "sw_image":
+        sc, rq = S.config_c1()
+        return [sc], [(0, rq)], ("SW image 64x64 x 32 spp, 1 band at 550 nm, 50 layers, cloud "
+                                 "32x32x16 lognormal")
+    if name == "cie_image":
+        sc, rq = S.config_c3(scale=256 / 512, spp=16, cloud_def=(128, 128, 32))
+        return [sc], [(0, rq)], ("CIE image 256x256 x 16 spp x 3 channels, 30 bands x 16 quad, cloud "
+                                 "128x128x32 power-law (CIE config at 1/2 side, 1/4 spp, 1/8 cloud)")
+    scenes = S.batched_scenes(scale=0.25)
+    reqs = S.batched_requests(n=24, side_range=(16, 96), spp_range=(16, 128))
+    return scenes, reqs, ("24 uneven requests (side log-U[16,96], spp log-U[16,128], 50% SW / 50% LW "
+                          "images) on 3 cloud scenes (32^3, 64x64x16, 128x128x32) in one launch")
 
 
-def cpu_baseline(scene, req, seconds: float):
+def cpu_baseline(scenes, reqs, seconds: float):
     """The oracle (CPU restatement of the reference path, OpenMP over all host
-    cores) on a bounded sample of the map: probe rows are added until the
-    sample takes about `seconds`."""
+    cores) on a bounded sample of the workload: pixel rows of the first request
+    are added until the sample takes about `seconds`."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    os_ = O.OracleScene(scene, O.props_for_mode(req.mode))
+    isc, req = reqs[0]
+    os_ = O.OracleScene(scenes[isc], O.props_for_mode(req.mode))
     npix = req.width * req.height
-    rows = 1
-    done_real, spent = 0, 0.0
-    begin = 0
-    while spent < seconds and begin < npix:
+    rows, begin, done_real, spent, rounds = 1, 0, 0, 0.0, 0
+    while spent < seconds and rounds < 64:
         end = min(npix, begin + rows * req.width)
         t0 = time.perf_counter()
         _, cnt = os_.draw_map(req, begin, end, nthreads=cores)
-        dt = time.perf_counter() - t0
+        spent += time.perf_counter() - t0
         done_real += cnt["nreal"]
-        spent += dt
-        begin = end
+        begin = 0 if end >= npix else end
         rows *= 2
-    if begin >= npix and spent < seconds:
-        pass
+        rounds += 1
     os_.close()
     return {"value": done_real / spent / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done_real} realisations = the first {begin} of {npix} probes x {req.spp} "
-                      f"in {spent:.1f} s (oracle, FP64, OpenMP)"}
+            "sample": f"{done_real} realisations of the first request's pixels, in {spent:.1f} s "
+                      f"(oracle, FP64 transport, OpenMP)"}
 
 
 def run_reference(args):
-    rank, world, _ = dist_env()
+    rank, _, _ = dist_env()
     if rank != 0:
         return
-    scene, req = workload()
     from oracle import oracle as O
+    scenes, reqs, desc = workload(args.workload)
+    isc, req = reqs[0]
     cores = os.cpu_count() or 1
-    os_ = O.OracleScene(scene, O.props_for_mode(req.mode))
+    os_ = O.OracleScene(scenes[isc], O.props_for_mode(req.mode))
     npix = req.width * req.height
-    # each step: a bounded sample of probe rows sized to about 2 s
     t0 = time.perf_counter()
-    _, cnt = os_.draw_map(req, 0, 8 * req.width, nthreads=cores)
-    probe = time.perf_counter() - t0
-    rows = max(1, min(req.height, int(8 * 2.0 / max(probe, 1e-3))))
-    end = rows * req.width
+    os_.draw_map(req, 0, min(npix, 8 * req.width), nthreads=cores)
+    probe = max(time.perf_counter() - t0, 1e-3)
+    rows = max(1, min(req.height, int(8 * 2.0 / probe)))  # each step ~2 s of CPU work
+    end = min(npix, rows * req.width)
     for _ in range(args.warmup):
         os_.draw_map(req, 0, min(end, 8 * req.width), nthreads=cores)
     times, reals = [], 0
@@ -179,18 +200,17 @@ def run_reference(args):
         reals += cnt["nreal"]
     total = sum(times)
     value = reals / total / 1e6
-    line = {
+    print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": "LW flux map 128x128 probes x 256 realisations, 16 bands x 8 quad, "
-                               "cloud 64x64x32 repeated", "sample_probes": end},
+        "config": {"workload": desc, "sample_pixels_per_step": end},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"first {end} of {npix} probes x {req.spp} realisations per step"},
+                         "sample": f"first {end} of {npix} pixels x {req.realisations_per_pixel} "
+                                   f"realisations per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+    }), flush=True)
 
 
 def main():
@@ -210,58 +230,78 @@ def main():
 
     from htrdr_kmin_b200 import api, build
     build.build()
-    scene, req = workload()
-    req.seed = 1000 + rank  # independent streams per rank (weak scaling)
-    gs = api.GpuScene(scene, api.props_for_mode(req.mode), device=local)
-    npix = req.width * req.height
-    dt = api.pixel_dtype(req.mode)
-    dev_out = torch.empty(npix * dt.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
-    host_out = torch.empty(npix * dt.itemsize, dtype=torch.uint8, pin_memory=True)
-
-    r = api.to_request(req)
-    lay = api.layout_for(req)
     L = api.lib()
-    import ctypes as C
+    scenes, reqs, desc = workload(args.workload)
+    for _, r in reqs:
+        r.seed = r.seed * 1000 + rank  # independent streams per rank (weak scaling)
+    need = [0] * len(scenes)
+    for isc, r in reqs:
+        need[isc] |= api.props_for_mode(r.mode)
+    gss = [api.GpuScene(s, need[i], device=local) for i, s in enumerate(scenes)]
+    n = len(reqs)
+    dev = [torch.empty(r.width * r.height * api.pixel_dtype(r.mode).itemsize, dtype=torch.uint8,
+                       device=f"cuda:{local}") for _, r in reqs]
+    host = [torch.empty(d.numel(), dtype=torch.uint8, pin_memory=True) for d in dev]
+    creq = [api.to_request(r) for _, r in reqs]
+    clay = [api.layout_for(r) for _, r in reqs]
+    items_dev = (api.BatchItem * n)()
+    items_host = (api.BatchItem * n)()
+    for i, (isc, _) in enumerate(reqs):
+        for arr, buf in ((items_dev, dev[i].data_ptr()), (items_host, host[i].data_ptr())):
+            arr[i].scene = gss[isc].handle.value
+            arr[i].req = creq[i]
+            arr[i].layout = clay[i]
+            arr[i].buffer = buf
+    total_real = sum(r.realisations for _, r in reqs)
+
+    def check(res, what):
+        if res != 0:
+            raise api.HtrdrError(what, res, L.htrdr_gpu_last_error().decode())
+
+    # block size, queue chunk and regroup period from the autotuner (untimed)
+    tuning, _ = api.autotune(items_dev)
 
     def step_batched():
-        """The batched persistent kernel, output left in HBM."""
-        item = (api.BatchItem * 1)()
-        item[0].scene = gs.handle.value
-        item[0].req = r
-        item[0].layout = lay
-        item[0].buffer = dev_out.data_ptr()
+        """all requests in one persistent launch, outputs left in HBM"""
         st = api.Stats()
-        res = L.htrdr_gpu_draw_maps_batched_device(item, 1, None, C.byref(st))
-        if res != 0:
-            raise api.HtrdrError("draw_maps_batched_device", res)
+        check(L.htrdr_gpu_draw_maps_batched_device(items_dev, n, C.byref(tuning), C.byref(st)),
+              "batched_device")
         return st
 
-    def step_device():
-        st = api.Stats()
-        res = L.htrdr_gpu_draw_map_device(gs.handle, C.byref(r), C.byref(lay),
-                                          C.c_void_p(dev_out.data_ptr()), C.byref(st))
-        if res != 0:
-            raise api.HtrdrError("draw_map_device", res)
-        return st
+    def step_plain():
+        """the plain drop-in kernel, one launch per request"""
+        k = 0.0
+        for i, (isc, _) in enumerate(reqs):
+            st = api.Stats()
+            check(L.htrdr_gpu_draw_map_device(gss[isc].handle, C.byref(creq[i]), C.byref(clay[i]),
+                                              C.c_void_p(dev[i].data_ptr()), C.byref(st)), "draw_map_device")
+            k += st.kernel_ms
+        return k
 
-    def step_host():
-        st = api.Stats()
-        res = L.htrdr_gpu_draw_map(gs.handle, C.byref(r), C.byref(lay),
-                                   C.c_void_p(host_out.data_ptr()), C.byref(st))
-        if res != 0:
-            raise api.HtrdrError("draw_map", res)
-        return st
+    def step_e2e():
+        """through the C ABI into pinned host buffers"""
+        if n == 1:
+            st = api.Stats()
+            check(L.htrdr_gpu_draw_map(gss[reqs[0][0]].handle, C.byref(creq[0]), C.byref(clay[0]),
+                                       C.c_void_p(host[0].data_ptr()), C.byref(st)), "draw_map")
+        else:
+            st = api.Stats()
+            check(L.htrdr_gpu_draw_maps_batched(items_host, n, C.byref(tuning), C.byref(st)), "batched")
+
+    flux = [i for i, (_, r) in enumerate(reqs) if r.mode in (S.MODE_FLUX_SW, S.MODE_FLUX_LW)]
 
     def reduce_accumulators():
-        if dist is None:
+        """NCCL sum of the flux maps' FP64 accumulators on rank 0"""
+        if dist is None or not flux:
             return 0.0
-        words = dev_out.view(torch.float64).view(npix, 8)
-        f = words[:, [0, 1, 4, 5]].contiguous()
-        u = dev_out.view(torch.int64).view(npix, 8)[:, [2, 3, 6, 7]].contiguous()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        dist.reduce(f, dst=0, op=dist.ReduceOp.SUM)
-        dist.reduce(u, dst=0, op=dist.ReduceOp.SUM)
+        for i in flux:
+            npix = reqs[i][1].width * reqs[i][1].height
+            f = dev[i].view(torch.float64).view(npix, 8)[:, [0, 1, 4, 5]].contiguous()
+            u = dev[i].view(torch.int64).view(npix, 8)[:, [2, 3, 6, 7]].contiguous()
+            dist.reduce(f, dst=0, op=dist.ReduceOp.SUM)
+            dist.reduce(u, dst=0, op=dist.ReduceOp.SUM)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
@@ -271,13 +311,12 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    # the plain drop-in kernel on the same map (reported beside the batched one)
     for _ in range(args.warmup):
         step_batched()
-        step_device()
         reduce_accumulators()
+    step_plain()
     barrier()
-    ms_plain = [step_device().kernel_ms for _ in range(max(1, args.steps))]
+    plain_ms = step_plain()
 
     barrier()
     kernel_ms, total_ms, stats = [], [], []
@@ -292,11 +331,10 @@ def main():
         barrier()
     clocks = clk.summary()
 
-    # end-to-end through the C ABI with a pinned host buffer (wall clock)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        step_host()
+        step_e2e()
     barrier()
     e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
 
@@ -306,49 +344,51 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step_ms, e2e_ms = float(t[0]), float(t[1])
 
-    reals = stats[-1].realisations
-    value = world * reals / (step_ms * 1e-3) / 1e6
-    e2e_value = world * reals / (e2e_ms * 1e-3) / 1e6
     last = stats[-1]
+    reals = last.realisations
+    value = world * reals / (step_ms * 1e-3) / 1e6
     kms = float(np.mean(kernel_ms))
     alg_bytes = 16 * last.nodes + 8 * last.collisions + 32 * last.realisations
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kms * 1e-3) / 1e9
-    plain_value = reals / (np.mean(ms_plain) * 1e-3) / 1e6
+    out_bytes = sum(d.numel() for d in dev)
 
     if rank == 0:
-        cpu = None
-        if not args.no_cpu_baseline:
-            cpu = cpu_baseline(scene, req, args.cpu_sample_s)
+        cpu = None if args.no_cpu_baseline else cpu_baseline(scenes, reqs, args.cpu_sample_s)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene and probes)",
-            "config": {"workload": "LW flux map 128x128 probes x 256 realisations/probe, 16 bands x 8 "
-                                   "quad, 50 layers, cloud 64x64x32 repeated, batched persistent kernel",
-                       "realisations_per_step_per_gpu": int(reals),
-                       "l2": f"inputs larger than L2: scene {gs.device_bytes / 1e6:.0f} MB resident",
-                       "parallelism": f"replicated scene, ranks render independent streams, NCCL sum of "
-                                      f"FP64 accumulators" if world > 1 else "single GPU"},
+            "data": "synthetic (seeded scenes and sensors)",
+            "config": {"workload": desc + ", batched persistent kernel",
+                       "realisations_per_step_per_gpu": int(total_real),
+                       "tuning": {"block_size": tuning.block_size, "queue_chunk": tuning.queue_chunk,
+                                  "regroup_period": tuning.regroup_period, "from": "autotuner"},
+                       "l2": "inputs larger than L2: scenes of "
+                             f"{sum(g.device_bytes for g in gss) / 1e6:.0f} MB resident",
+                       "parallelism": ("replicated scene, independent streams per rank, NCCL sum of FP64 "
+                                       "accumulators") if world > 1 else "single GPU"},
             "clocks": clocks,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(C.sizeof(r) + C.sizeof(lay)),
-                    "d2h_bytes_per_step": int(npix * dt.itemsize)},
-            "gpu_launches": 2 * args.steps,
+            "e2e": {"value": world * reals / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": int(n * (C.sizeof(api.Request) + C.sizeof(api.BufferLayout))),
+                    "d2h_bytes_per_step": int(out_bytes)},
+            "gpu_launches": (1 + n) * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "peak_kind": peak_kind, "kernel": "k_persistent",
-                         "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": kms},
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_persistent", "alg_bytes_per_launch": int(alg_bytes),
+                         "kernel_ms": kms},
             "cpu_baseline": cpu,
-            "plain_gpu": {"value": plain_value, "unit": UNIT, "kernel": "k_plain",
-                          "kernel_ms": float(np.mean(ms_plain))},
+            "plain_gpu": {"value": reals / (plain_ms * 1e-3) / 1e6, "unit": UNIT, "kernel": "k_plain",
+                          "kernel_ms": plain_ms, "launches": n},
+            "batched_vs_plain": plain_ms / kms,
             "segments_per_s": last.segments / (kms * 1e-3),
             "counters": {"segments": last.segments, "nodes": last.nodes,
                          "collisions": last.collisions, "realisations": last.realisations,
                          "failures": last.failures},
         }
         print(json.dumps(line), flush=True)
-    gs.close()
+    for g in gss:
+        g.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -36,7 +36,7 @@ EXPORTED = [
     "htrdr_gpu_draw_map_device", "htrdr_gpu_radiance_sw", "htrdr_gpu_radiance_lw",
     "htrdr_gpu_realisation_weights", "htrdr_gpu_find_band", "htrdr_gpu_sample_quad",
     "htrdr_gpu_locate_leaf", "htrdr_gpu_sample_wavelength", "htrdr_gpu_draw_maps_batched",
-    "htrdr_gpu_draw_maps_batched_device",
+    "htrdr_gpu_draw_maps_batched_device", "htrdr_gpu_autotune",
     "htrdr_gpu_default_tuning", "htrdr_gpu_version", "htrdr_gpu_device_count",
     "htrdr_gpu_last_error",
 ]
@@ -149,6 +149,7 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_sample_wavelength.argtypes = [vp, C.POINTER(Request), i32, sz, dp, dp, up, dp, dp]
     L.htrdr_gpu_draw_maps_batched.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(Stats)]
     L.htrdr_gpu_draw_maps_batched_device.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(Stats)]
+    L.htrdr_gpu_autotune.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(C.c_double)]
     L.htrdr_gpu_default_tuning.argtypes = [C.POINTER(Tuning)]
     L.htrdr_gpu_default_tuning.restype = None
     L.htrdr_gpu_version.restype = C.c_char_p
@@ -377,6 +378,16 @@ def draw_maps_batched(items: Sequence[tuple], tuning: Optional[Tuning] = None):
     t = tuning if tuning is not None else default_tuning()
     _check(lib().htrdr_gpu_draw_maps_batched(arr, n, C.byref(t), C.byref(st)), "draw_maps_batched")
     return bufs, st.as_dict()
+
+
+def autotune(items_device) -> tuple:
+    """Pick the batched engine's tuning on a ctypes BatchItem array whose
+    buffers are device memory.  Returns (Tuning, best kernel ms)."""
+    t = Tuning()
+    ms = C.c_double()
+    _check(lib().htrdr_gpu_autotune(items_device, len(items_device), C.byref(t), C.byref(ms)),
+           "htrdr_gpu_autotune")
+    return t, ms.value
 
 
 def device_count() -> int:

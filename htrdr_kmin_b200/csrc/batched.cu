@@ -10,10 +10,11 @@
  * weight of each realisation is the same as in the one-thread-per-realisation
  * kernel because both run the same state machine on the same stream.
  *
- * Once the queue is empty the warps drain their live paths; every
- * `regroup_period' steps, lanes that are idle vote (warp ballot) and a warp
- * whose live paths are fewer than a quarter of its lanes hands them to the
- * block through shared memory, so that the tail runs on few, full warps. */
+ * Lanes are regrouped by warp ballot: lanes whose trace ended (scattering
+ * events, sun sampling, accumulation) and idle lanes (new realisations) wait
+ * and are served together once every `regroup_period' voxel steps, or as soon
+ * as no lane of the warp is tracing, so that the long sampling code runs with
+ * many lanes at once while the tracing lanes keep stepping. */
 #include "internal.h"
 #include "transport.cuh"
 
@@ -65,9 +66,23 @@ accumulate_b(const Path& p, const DRequest& R, DAccum* acc, DAccum* tacc)
   atomicAdd(&t->n, 1ull);
 }
 
-__global__ void __launch_bounds__(256)
-k_persistent(BatchTables B)
+__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
+k_persistent(BatchTables B, uint32_t nscenes, int tables_in_smem)
 {
+  /* the scene and request views are read on every step: keep them in shared
+   * memory when they fit (one copy per block) */
+  extern __shared__ __align__(16) unsigned char smem[];
+  if(tables_in_smem) {
+    DScene* ss = (DScene*)smem;
+    DRequest* sr = (DRequest*)(smem + ((nscenes * sizeof(DScene) + 15) & ~(size_t)15));
+    const uint32_t* gs = (const uint32_t*)B.scenes;
+    const uint32_t* gr = (const uint32_t*)B.reqs;
+    for(uint32_t i = threadIdx.x; i < nscenes * sizeof(DScene) / 4; i += blockDim.x) ((uint32_t*)ss)[i] = gs[i];
+    for(uint32_t i = threadIdx.x; i < B.nreq * sizeof(DRequest) / 4; i += blockDim.x) ((uint32_t*)sr)[i] = gr[i];
+    __syncthreads();
+    B.scenes = ss;
+    B.reqs = sr;
+  }
   const unsigned lane = threadIdx.x & 31u;
   Path p;
   p.state = ST_IDLE;
@@ -77,8 +92,19 @@ k_persistent(BatchTables B)
   uint64_t wcur = 0, wend = 0; /* private chunk of the queue */
   bool drained = false;
   unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
+  const uint32_t period = B.regroup_period > 1 ? B.regroup_period : 1;
 
-  for(;;) {
+  for(uint32_t it = 0;; ++it) {
+    /* Regrouping: lanes whose trace ended (events, accumulation) and idle
+     * lanes (new realisations) are served together once every `period'
+     * iterations, or as soon as no lane of the warp is tracing; in between,
+     * the tracing lanes advance alone, so that the long sensor-sampling and
+     * scattering code runs with many lanes at once. */
+    const unsigned tmask = __ballot_sync(0xffffffffu, p.state == ST_TRACE);
+    if(tmask && (it % period) != 0) {
+      if(p.state == ST_TRACE) trace_step(p, B.scenes[__ldg(B.req_scene + ri)]);
+      continue;
+    }
     /* refill the private chunk of lanes that are idle with nothing left */
     const bool need = p.state == ST_IDLE && wcur >= wend && !drained;
     const unsigned m = __ballot_sync(0xffffffffu, need);
@@ -156,7 +182,7 @@ htrdr_gpu_default_tuning(htrdr_gpu_tuning* t)
   if(!t) return;
   t->block_size = 128;
   t->queue_chunk = 4;
-  t->regroup_period = 0;
+  t->regroup_period = 1;
   t->blocks_per_sm = 0;
 }
 
@@ -237,9 +263,15 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
   B.chunk = tun.queue_chunk;
   B.regroup_period = tun.regroup_period;
 
+  static_assert(sizeof(DScene) % 4 == 0 && sizeof(DRequest) % 4 == 0, "word copies");
+  const size_t tables = ((scenes.size() * sizeof(DScene) + 15) & ~(size_t)15) + n * sizeof(DRequest);
+  const int in_smem = tables <= 96 * 1024;
+  const size_t smem = in_smem ? tables : 0;
+  if(smem > 48 * 1024)
+    cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int nsm = 0, per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)tun.block_size, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)tun.block_size, smem);
   if(tun.blocks_per_sm) per_sm = std::min(per_sm, (int)tun.blocks_per_sm);
   per_sm = std::max(per_sm, 1);
   const unsigned grid = (unsigned)(nsm * per_sm);
@@ -252,7 +284,7 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
   ok = ok && cuda_ok(cudaMemsetAsync(d_cnt.ptr, 0, 128, st), "memset");
   cudaEventRecord(e1, st);
   if(ok) {
-    k_persistent<<<grid, tun.block_size, 0, st>>>(B);
+    k_persistent<<<grid, tun.block_size, smem, st>>>(B, (uint32_t)scenes.size(), in_smem);
     ok = cuda_ok(cudaGetLastError(), "k_persistent");
   }
   cudaEventRecord(e2, st);
@@ -291,4 +323,35 @@ htrdr_gpu_draw_maps_batched_device(htrdr_gpu_batch_item* items, size_t n,
                                    const htrdr_gpu_tuning* tuning, htrdr_gpu_stats* stats)
 {
   return batched_impl(items, n, tuning, stats, false);
+}
+
+/* Autotuner of the batched engine: times every candidate (block size x queue
+ * chunk x regroup period) on the given items (device buffers) with CUDA
+ * events and returns the fastest.  Results do not depend on the tuning. */
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best, double* best_ms)
+{
+  if(!items || !n || !best) return HTRDR_GPU_RES_BAD_ARG;
+  static const uint32_t blocks[] = {128, 256};
+  static const uint32_t chunks[] = {1, 4};
+  static const uint32_t periods[] = {1, 4, 16, 64};
+  htrdr_gpu_stats st;
+  double best_t = 1e300;
+  htrdr_gpu_tuning t;
+  htrdr_gpu_default_tuning(&t);
+  htrdr_gpu_res_T res = batched_impl(items, n, &t, &st, false); /* warm-up */
+  if(res != HTRDR_GPU_RES_OK) return res;
+  for(uint32_t b : blocks)
+    for(uint32_t c : chunks)
+      for(uint32_t p : periods) {
+        t.block_size = b;
+        t.queue_chunk = c;
+        t.regroup_period = p;
+        t.blocks_per_sm = 0;
+        res = batched_impl(items, n, &t, &st, false);
+        if(res != HTRDR_GPU_RES_OK) return res;
+        if(st.kernel_ms < best_t) { best_t = st.kernel_ms; *best = t; }
+      }
+  if(best_ms) *best_ms = best_t;
+  return HTRDR_GPU_RES_OK;
 }

@@ -13,6 +13,15 @@
 #define HG_MAX_BOUNCES (1u << 16) /* scattering events per realisation before giving up */
 #define HG_MAX_NULL (1u << 22)    /* tentative collisions per voxel before giving up */
 
+/* Register budget of the transport kernels (per thread): trades occupancy
+ * against spills of the per-path state. */
+#ifndef HG_PLAIN_MAXNREG
+#define HG_PLAIN_MAXNREG 168
+#endif
+#ifndef HG_PERSIST_MAXNREG
+#define HG_PERSIST_MAXNREG 255
+#endif
+
 enum { HG_KA = 0, HG_KS = 1, HG_KEXT = 2 };
 enum { HG_XWAVE_SW = 0, HG_XWAVE_LW = 1, HG_IMAGE_CIE = 2, HG_FLUX_SW = 3, HG_FLUX_LW = 4 };
 
@@ -23,6 +32,8 @@ struct DScene {
   const float* layer_T;   /* [nlayers] */
   float ztop;
   const float2* gas;      /* [nq][nlayers] {ka, ks} */
+  const double* layer_zd; /* [nlayers+1] layer bounds, FP64 */
+  const double* gas_cum;  /* [nq][3][nlayers+1] cumulative vertical optical depth from z = 0 */
   /* spectral */
   uint32_t nbands;
   const double* band_lo;  /* [nbands] */
@@ -62,6 +73,8 @@ struct DRequest {
   const double* cdf;     /* Planck: [ncdf]; CIE: [3][ncdf] */
   const double* pdf;     /* Planck: [ncdf] */
   const double* fbound;  /* CIE: [3][ncdf][2] fit values at each band's bounds */
+  const uint32_t* guide; /* [nch][nguide+1]: first CDF entry >= b/nguide (may be null) */
+  uint32_t nguide;       /* power of two */
   double rcp_integral[3];
   double ref_T;
   /* camera */

@@ -37,7 +37,8 @@ struct Sampler {
   uint32_t ncdf = 0;
   double band_len = 0;
   double rcp_integral[3] = {0, 0, 0};
-  DevBuf cdf, pdf, fbound;
+  DevBuf cdf, pdf, fbound, guide;
+  uint32_t nguide = 0;
   std::vector<double> host_cdf; /* for the host-side checks */
 };
 

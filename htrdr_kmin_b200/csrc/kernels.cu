@@ -58,7 +58,7 @@ flush_counters(Counters* cnt, unsigned long long seg, unsigned long long node,
   }
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __maxnreg__(HG_PLAIN_MAXNREG)
 k_plain(DScene S, DRequest R, DAccum* acc, DAccum* tacc, uint64_t pix_begin, uint32_t npix,
         double* weights, Counters* cnt)
 {

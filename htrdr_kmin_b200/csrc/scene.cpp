@@ -337,6 +337,23 @@ scene_sampler(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, htrdr_gpu_res_
       s->host_cdf = cdf;
     }
   }
+  if(s->ncdf) { /* guide table: first CDF entry >= b/G for b = 0..G */
+    const uint32_t nch = cie ? 3u : 1u;
+    const uint32_t G = cie ? 1024u : 16384u;
+    std::vector<uint32_t> g((size_t)nch * (G + 1));
+    for(uint32_t ch = 0; ch < nch; ++ch) {
+      const double* c = s->host_cdf.data() + (size_t)ch * s->ncdf;
+      for(uint32_t b = 0; b <= G; ++b) {
+        const double key = (double)b / (double)G;
+        g[(size_t)ch * (G + 1) + b] = (uint32_t)(std::lower_bound(c, c + s->ncdf, key) - c);
+      }
+    }
+    if(!s->guide.upload(g.data(), g.size() * 4)) {
+      *res = HTRDR_GPU_RES_MEM_ERR;
+      return nullptr;
+    }
+    s->nguide = G;
+  }
   Sampler* raw = s.get();
   scn->samplers.emplace(key, std::move(s));
   return raw;
@@ -377,6 +394,8 @@ make_drequest(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, DRequest* R)
   R->cdf = (const double*)smp->cdf.ptr;
   R->pdf = (const double*)smp->pdf.ptr;
   R->fbound = (const double*)smp->fbound.ptr;
+  R->guide = (const uint32_t*)smp->guide.ptr;
+  R->nguide = smp->nguide;
   for(int i = 0; i < 3; ++i) R->rcp_integral[i] = smp->rcp_integral[i];
   R->ref_T = req->ref_temperature;
   /* perspective / orthographic camera (star-camera) */
@@ -500,10 +519,27 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
     return p;
   };
 
+  /* cumulative vertical optical depth of the gas column per (quad, property):
+   * cum[l] = sum_{i<l} k_i (z_{i+1} - z_i), with k the single-precision
+   * coefficient the voxel-by-voxel traversal would use */
+  std::vector<double> cum_tau((size_t)nq * 3 * (nl + 1));
+  for(uint32_t q = 0; q < nq; ++q) {
+    for(int p = 0; p < 3; ++p) {
+      double* c = &cum_tau[((size_t)q * 3 + p) * (nl + 1)];
+      c[0] = 0.0;
+      for(uint32_t l = 0; l < nl; ++l) {
+        const float a = desc->gas_ka[(size_t)q * nl + l], s = desc->gas_ks[(size_t)q * nl + l];
+        const float k = p == HG_KA ? a : (p == HG_KS ? s : a + s);
+        c[l + 1] = c[l] + (double)k * (desc->layer_z[l + 1] - desc->layer_z[l]);
+      }
+    }
+  }
   S.nlayers = nl;
   S.ztop = lz[nl];
   S.nbands = nb;
-  if(!(S.layer_z = (const float*)upload(lz.data(), lz.size() * 4))
+  if(!(S.layer_zd = (const double*)upload(desc->layer_z, (nl + 1) * 8))
+  || !(S.gas_cum = (const double*)upload(cum_tau.data(), cum_tau.size() * 8))
+  || !(S.layer_z = (const float*)upload(lz.data(), lz.size() * 4))
   || !(S.layer_T = (const float*)upload(lT.data(), lT.size() * 4))
   || !(S.gas = (const float2*)upload(gas.data(), gas.size() * 8))
   || !(S.band_lo = (const double*)upload(desc->band_lo, nb * 8))

@@ -362,10 +362,11 @@ def batched_scenes(scale: float = 1.0) -> List[Scene]:
         ssa = np.array([0.999] * 4 + [0.5] * 4, dtype=np.float32)
         g = np.full(8, 0.85, dtype=np.float32)
         cell = 6400.0 / max(nx, ny) if scale != 1.0 else 50.0
+        dz = 1000.0 / nz  # a 1 km thick cloud layer based at 1 km
         scenes.append(Scene(layer_z=layer_z, layer_T=temperature_profile(layer_z),
                             band_lo=band_lo, band_hi=band_hi, nquads=nquads, quad_w=w,
                             gas_ka=ka, gas_ks=ks, cloud_lwc=lwc,
-                            cloud_lower=(0.0, 0.0, 1000.0), cloud_cell=(cell, cell, cell),
+                            cloud_lower=(0.0, 0.0, 1000.0), cloud_cell=(cell, cell, dz),
                             cloud_sigma_ext=sig, cloud_ssa=ssa, cloud_g=g,
                             repeat_clouds=True, ground_reflectivity=0.2,
                             sun_azimuth=45.0, sun_elevation=50.0,

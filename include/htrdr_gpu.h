@@ -210,7 +210,8 @@ struct htrdr_gpu_batch_item {
 struct htrdr_gpu_tuning {
   uint32_t block_size;    /* threads per block of the persistent kernel */
   uint32_t queue_chunk;   /* realisations taken from the work queue at once */
-  uint32_t regroup_period;/* transport steps between two live-path regroupings */
+  uint32_t regroup_period;/* voxel steps between two regroupings of a warp's lanes (events and
+                           * new realisations run together; 0 or 1: every step) */
   uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
 };
 /* Renders every item (each one htrdr_draw_map call of the reference) in one
@@ -224,6 +225,12 @@ htrdr_gpu_draw_maps_batched_device(struct htrdr_gpu_batch_item* items, size_t n,
                                    const struct htrdr_gpu_tuning* tuning,
                                    struct htrdr_gpu_stats* stats);
 HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
+/* Autotuner: times the candidate tunings (block size, queue chunk, regroup
+ * period) of the batched engine on `items' (device buffers) and returns the
+ * fastest; the rendered values do not depend on the tuning. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_autotune(struct htrdr_gpu_batch_item* items, size_t n, struct htrdr_gpu_tuning* best,
+                   double* best_ms);
 
 /* ---- library info ---- */
 HTRDR_GPU_API const char* htrdr_gpu_version(void);
