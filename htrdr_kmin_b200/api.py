@@ -36,7 +36,10 @@ EXPORTED = [
     "htrdr_gpu_draw_map_device", "htrdr_gpu_radiance_sw", "htrdr_gpu_radiance_lw",
     "htrdr_gpu_realisation_weights", "htrdr_gpu_find_band", "htrdr_gpu_sample_quad",
     "htrdr_gpu_locate_leaf", "htrdr_gpu_sample_wavelength", "htrdr_gpu_draw_maps_batched",
-    "htrdr_gpu_draw_maps_batched_device", "htrdr_gpu_autotune",
+    "htrdr_gpu_draw_maps_batched_device", "htrdr_gpu_autotune", "htrdr_gpu_batch_create",
+    "htrdr_gpu_batch_run", "htrdr_gpu_batch_release", "htrdr_gpu_server_create",
+    "htrdr_gpu_server_submit", "htrdr_gpu_server_poll", "htrdr_gpu_server_wait",
+    "htrdr_gpu_server_stats", "htrdr_gpu_server_release",
     "htrdr_gpu_default_tuning", "htrdr_gpu_version", "htrdr_gpu_device_count",
     "htrdr_gpu_last_error",
 ]
@@ -103,6 +106,22 @@ class BatchItem(C.Structure):
                 ("buffer", C.c_void_p)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t),
+                ("round_target_ms", C.c_double), ("round_realisations", C.c_uint64),
+                ("tuning", Tuning)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("rounds", C.c_uint64), ("realisations", C.c_uint64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+                ("busy_ms", C.c_double), ("wall_ms", C.c_double), ("hbm_peak_bytes", C.c_size_t)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 PIXEL_XWAVE = np.dtype([("L", "<f8"), ("L_se", "<f8"), ("Tb", "<f8"), ("Tb_se", "<f8"),
                         ("t_sum", "<f8"), ("t_sum2", "<f8"), ("t_n", "<u8"), ("t_nfail", "<u8")])
 PIXEL_FLUX = np.dtype([("sum", "<f8"), ("sum2", "<f8"), ("n", "<u8"), ("nfail", "<u8"),
@@ -150,6 +169,18 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_draw_maps_batched.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(Stats)]
     L.htrdr_gpu_draw_maps_batched_device.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(Stats)]
     L.htrdr_gpu_autotune.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(C.c_double)]
+    L.htrdr_gpu_batch_create.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(C.c_void_p)]
+    L.htrdr_gpu_batch_run.argtypes = [vp, C.POINTER(Stats)]
+    L.htrdr_gpu_batch_release.argtypes = [vp]
+    L.htrdr_gpu_batch_release.restype = None
+    L.htrdr_gpu_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]
+    L.htrdr_gpu_server_submit.argtypes = [vp, vp, C.POINTER(Request), C.POINTER(BufferLayout), vp,
+                                          C.POINTER(C.c_uint64)]
+    L.htrdr_gpu_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.htrdr_gpu_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(C.c_int)]
+    L.htrdr_gpu_server_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    L.htrdr_gpu_server_release.argtypes = [vp]
+    L.htrdr_gpu_server_release.restype = None
     L.htrdr_gpu_default_tuning.argtypes = [C.POINTER(Tuning)]
     L.htrdr_gpu_default_tuning.restype = None
     L.htrdr_gpu_version.restype = C.c_char_p
@@ -388,6 +419,67 @@ def autotune(items_device) -> tuple:
     _check(lib().htrdr_gpu_autotune(items_device, len(items_device), C.byref(t), C.byref(ms)),
            "htrdr_gpu_autotune")
     return t, ms.value
+
+
+class Server:
+    """Request loop with continuous batching (htrdr_gpu_server_*).
+
+    ``submit`` returns a ticket; the map lands in a NumPy buffer returned by
+    ``result`` once ``wait``/``poll`` report completion."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 150 << 30,
+                 round_target_ms: float = 20.0, round_realisations: int = 0,
+                 tuning: Optional[Tuning] = None):
+        cfg = ServerConfig()
+        cfg.device = device
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        cfg.round_target_ms = round_target_ms
+        cfg.round_realisations = round_realisations
+        cfg.tuning = tuning if tuning is not None else default_tuning()
+        h = C.c_void_p()
+        _check(lib().htrdr_gpu_server_create(C.byref(cfg), C.byref(h)), "htrdr_gpu_server_create")
+        self.handle = h
+        self._bufs = {}
+
+    def submit(self, scene: "GpuScene", req: S.Request) -> int:
+        buf = np.zeros((req.height, req.width), dtype=pixel_dtype(req.mode))
+        r = to_request(req)
+        lay = layout_for(req)
+        t = C.c_uint64()
+        _check(lib().htrdr_gpu_server_submit(self.handle, scene.handle, C.byref(r), C.byref(lay),
+                                             _ptr(buf), C.byref(t)), "htrdr_gpu_server_submit")
+        self._bufs[t.value] = buf
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        done, res = C.c_int(), C.c_int()
+        _check(lib().htrdr_gpu_server_poll(self.handle, ticket, C.byref(done), C.byref(res)), "poll")
+        if done.value and res.value != RES_OK:
+            raise HtrdrError("request", res.value)
+        return bool(done.value)
+
+    def wait(self, ticket: int, timeout_s: float = 600.0) -> np.ndarray:
+        res = C.c_int()
+        _check(lib().htrdr_gpu_server_wait(self.handle, ticket, timeout_s, C.byref(res)), "wait")
+        if res.value != RES_OK:
+            raise HtrdrError("request", res.value)
+        return self._bufs.pop(ticket)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().htrdr_gpu_server_stats(self.handle, C.byref(st)), "stats")
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().htrdr_gpu_server_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def device_count() -> int:

@@ -1,20 +1,25 @@
 /* Batched engine: many draw_map requests (images, flux maps, spectral
  * domains, scenes) in ONE persistent kernel fed by a device work queue.
  *
- * The realisations of all requests form one index space (request-major,
- * then realisation-major inside a request).  Each resident thread owns one
- * path slot; when its path ends it takes the next realisation from its
- * private chunk of the queue, refilled `queue_chunk` realisations at a time
- * by one warp-aggregated atomic.  Paths of very different lengths therefore
- * never leave lanes idle while work remains (path regeneration), and the
- * weight of each realisation is the same as in the one-thread-per-realisation
- * kernel because both run the same state machine on the same stream.
+ * A launch covers items -- ranges of realisations of requests -- whose
+ * realisations form one index space (item-major, realisation-major inside a
+ * request).  Each resident thread owns one path slot; when its path ends it
+ * takes the next realisation from its private chunk of the queue, refilled
+ * `queue_chunk' realisations at a time by one warp-aggregated atomic.  Paths
+ * of very different lengths therefore never leave lanes idle while work
+ * remains (path regeneration), and the weight of each realisation is the same
+ * as in the one-thread-per-realisation kernel because both run the same state
+ * machine on the same stream.
  *
  * Lanes are regrouped by warp ballot: lanes whose trace ended (scattering
  * events, sun sampling, accumulation) and idle lanes (new realisations) wait
  * and are served together once every `regroup_period' voxel steps, or as soon
  * as no lane of the warp is tracing, so that the long sampling code runs with
- * many lanes at once while the tracing lanes keep stepping. */
+ * many lanes at once while the tracing lanes keep stepping.
+ *
+ * Entry points: one-shot htrdr_gpu_draw_maps_batched(_device), the reusable
+ * htrdr_gpu_batch_* object whose launch sequence is captured once in a CUDA
+ * graph and replayed, and the autotuner. */
 #include "internal.h"
 #include "transport.cuh"
 
@@ -23,86 +28,66 @@
 
 namespace hg {
 
-struct BatchTables {
-  const DScene* scenes;       /* [nscenes] */
-  const DRequest* reqs;       /* [nreq] */
-  const uint32_t* req_scene;  /* [nreq] */
-  const uint64_t* offsets;    /* [nreq+1] prefix sums of realisations */
-  uint32_t nreq;
-  uint64_t total;
-  unsigned long long* next;   /* queue head */
-  DAccum* acc;
-  DAccum* tacc;
-  Counters* cnt;
-  uint32_t chunk;
-  uint32_t regroup_period;
-};
-
 __device__ __forceinline__ uint32_t
-find_request(const BatchTables& B, uint64_t g)
+find_item(const PTables& T, uint64_t g)
 {
-  uint32_t lo = 0, hi = B.nreq; /* last request whose offset <= g */
+  uint32_t lo = 0, hi = T.nitems; /* last item whose offset <= g */
   while(hi - lo > 1) {
     const uint32_t mid = (lo + hi) >> 1;
-    if(__ldg(B.offsets + mid) <= g) lo = mid; else hi = mid;
+    if(__ldg(T.offsets + mid) <= g) lo = mid; else hi = mid;
   }
   return lo;
 }
 
 __device__ __forceinline__ void
-accumulate_b(const Path& p, const DRequest& R, DAccum* acc, DAccum* tacc)
+accumulate_b(const Path& p, const DRequest& R)
 {
   if(p.flags & PF_REJECTED) return;
   const uint32_t nch = R.mode == HG_IMAGE_CIE ? 3u : 1u;
-  DAccum* a = acc + R.acc_base + (size_t)p.pix * nch + p.chan;
+  DAccum* a = R.acc + (size_t)p.pix * nch + p.chan;
   if(p.flags & PF_FAILED) { atomicAdd(&a->pad, 1ull); return; }
   atomicAdd(&a->s, p.weight);
   atomicAdd(&a->s2, p.weight * p.weight);
   atomicAdd(&a->n, 1ull);
   const double us = (double)(gtimer() - p.t0) * 1e-3;
-  DAccum* t = tacc + R.tacc_base + p.pix;
+  DAccum* t = R.tacc + p.pix;
   atomicAdd(&t->s, us);
   atomicAdd(&t->s2, us * us);
   atomicAdd(&t->n, 1ull);
 }
 
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
-k_persistent(BatchTables B, uint32_t nscenes, int tables_in_smem)
+k_persistent(PTables T, int tables_in_smem)
 {
   /* the scene and request views are read on every step: keep them in shared
    * memory when they fit (one copy per block) */
   extern __shared__ __align__(16) unsigned char smem[];
   if(tables_in_smem) {
     DScene* ss = (DScene*)smem;
-    DRequest* sr = (DRequest*)(smem + ((nscenes * sizeof(DScene) + 15) & ~(size_t)15));
-    const uint32_t* gs = (const uint32_t*)B.scenes;
-    const uint32_t* gr = (const uint32_t*)B.reqs;
-    for(uint32_t i = threadIdx.x; i < nscenes * sizeof(DScene) / 4; i += blockDim.x) ((uint32_t*)ss)[i] = gs[i];
-    for(uint32_t i = threadIdx.x; i < B.nreq * sizeof(DRequest) / 4; i += blockDim.x) ((uint32_t*)sr)[i] = gr[i];
+    DRequest* sr = (DRequest*)(smem + ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15));
+    const uint32_t* gs = (const uint32_t*)T.scenes;
+    const uint32_t* gr = (const uint32_t*)T.reqs;
+    for(uint32_t i = threadIdx.x; i < T.nscenes * sizeof(DScene) / 4; i += blockDim.x) ((uint32_t*)ss)[i] = gs[i];
+    for(uint32_t i = threadIdx.x; i < T.nreqs * sizeof(DRequest) / 4; i += blockDim.x) ((uint32_t*)sr)[i] = gr[i];
     __syncthreads();
-    B.scenes = ss;
-    B.reqs = sr;
+    T.scenes = ss;
+    T.reqs = sr;
   }
   const unsigned lane = threadIdx.x & 31u;
   Path p;
   p.state = ST_IDLE;
   p.flags = 0;
   p.c_seg = p.c_node = p.c_tc = 0;
-  uint32_t ri = 0;            /* request of the current path */
+  uint32_t ri = 0, si = 0;     /* request and scene of the current path */
   uint64_t wcur = 0, wend = 0; /* private chunk of the queue */
   bool drained = false;
   unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
-  const uint32_t period = B.regroup_period > 1 ? B.regroup_period : 1;
+  const uint32_t period = T.regroup_period > 1 ? T.regroup_period : 1;
 
   for(uint32_t it = 0;; ++it) {
-    /* Regrouping: lanes whose trace ended (events, accumulation) and idle
-     * lanes (new realisations) are served together once every `period'
-     * iterations, or as soon as no lane of the warp is tracing; in between,
-     * the tracing lanes advance alone, so that the long sensor-sampling and
-     * scattering code runs with many lanes at once. */
     const unsigned tmask = __ballot_sync(0xffffffffu, p.state == ST_TRACE);
-    if(tmask && (it % period) != 0) {
-      if(p.state == ST_TRACE) trace_step(p, B.scenes[__ldg(B.req_scene + ri)]);
+    if(tmask && (it % period) != 0) { /* not a regrouping step: tracing lanes only */
+      if(p.state == ST_TRACE) trace_step(p, T.scenes[si]);
       continue;
     }
     /* refill the private chunk of lanes that are idle with nothing left */
@@ -111,21 +96,24 @@ k_persistent(BatchTables B, uint32_t nscenes, int tables_in_smem)
     if(m) {
       const unsigned leader = __ffs(m) - 1;
       unsigned long long base = 0;
-      if(lane == leader) base = atomicAdd(B.next, (unsigned long long)__popc(m) * B.chunk);
+      if(lane == leader) base = atomicAdd(T.next, (unsigned long long)__popc(m) * T.chunk);
       base = __shfl_sync(0xffffffffu, base, leader);
       if(need) {
         const unsigned rank = __popc(m & ((1u << lane) - 1u));
-        wcur = base + (unsigned long long)rank * B.chunk;
-        wend = wcur + B.chunk;
-        if(wend > B.total) wend = B.total;
-        if(wcur >= B.total) { drained = true; wcur = wend = B.total; }
+        wcur = base + (unsigned long long)rank * T.chunk;
+        wend = wcur + T.chunk;
+        if(wend > T.total) wend = T.total;
+        if(wcur >= T.total) { drained = true; wcur = wend = T.total; }
       }
     }
     if(p.state == ST_IDLE && wcur < wend) {
       const uint64_t g = wcur++;
-      ri = find_request(B, g);
-      const DRequest& R = B.reqs[ri];
-      const uint64_t local = g - __ldg(B.offsets + ri);
+      const uint32_t ii = find_item(T, g);
+      const PItem item = T.items[ii];
+      ri = item.req;
+      si = item.scene;
+      const DRequest& R = T.reqs[ri];
+      const uint64_t local = g - __ldg(T.offsets + ii) + item.begin;
       const uint32_t npix = R.width * R.height;
       p.ireal = (uint32_t)(local / npix);
       p.pix = (uint32_t)(local % npix);
@@ -133,8 +121,8 @@ k_persistent(BatchTables B, uint32_t nscenes, int tables_in_smem)
     }
     if(!__any_sync(0xffffffffu, p.state != ST_IDLE)) break;
     if(p.state != ST_IDLE) {
-      const DRequest& R = B.reqs[ri];
-      const DScene& S = B.scenes[__ldg(B.req_scene + ri)];
+      const DRequest& R = T.reqs[ri];
+      const DScene& S = T.scenes[si];
       if(p.state != ST_TRACE && p.state != ST_DONE) {
         path_event(p, S, R);
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
@@ -143,7 +131,7 @@ k_persistent(BatchTables B, uint32_t nscenes, int tables_in_smem)
       if(p.state == ST_TRACE) {
         trace_step(p, S);
       } else if(p.state == ST_DONE) {
-        accumulate_b(p, R, B.acc, B.tacc);
+        accumulate_b(p, R);
         real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
         fail += (p.flags & PF_FAILED) ? 1 : 0;
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
@@ -161,16 +149,176 @@ k_persistent(BatchTables B, uint32_t nscenes, int tables_in_smem)
     fail += __shfl_down_sync(0xffffffffu, fail, o);
   }
   if(lane == 0) {
-    atomicAdd(&B.cnt->seg, seg);
-    atomicAdd(&B.cnt->node, node);
-    atomicAdd(&B.cnt->tc, tc);
-    atomicAdd(&B.cnt->real, real);
-    atomicAdd(&B.cnt->fail, fail);
+    Counters* c = (Counters*)T.cnt;
+    atomicAdd(&c->seg, seg);
+    atomicAdd(&c->node, node);
+    atomicAdd(&c->tc, tc);
+    atomicAdd(&c->real, real);
+    atomicAdd(&c->fail, fail);
   }
 }
 
-cudaError_t launch_finalize(const DRequest& R, const DAccum* acc, const DAccum* tacc, void* out,
-                            size_t pitch, cudaStream_t st);
+bool
+valid_tuning(const htrdr_gpu_tuning& t)
+{
+  return t.block_size && t.block_size <= 512 && !(t.block_size & 31) && t.queue_chunk;
+}
+
+cudaError_t
+launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm, int device,
+                  cudaStream_t st)
+{
+  static_assert(sizeof(DScene) % 4 == 0 && sizeof(DRequest) % 4 == 0, "word copies");
+  if(!T.total) return cudaSuccess;
+  const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
+  const int in_smem = tables <= 96 * 1024;
+  const size_t smem = in_smem ? tables : 0;
+  if(smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+    if(e != cudaSuccess) return e;
+  }
+  int nsm = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)block_size, smem);
+  if(blocks_per_sm) per_sm = std::min(per_sm, (int)blocks_per_sm);
+  per_sm = std::max(per_sm, 1);
+  k_persistent<<<(unsigned)(nsm * per_sm), block_size, smem, st>>>(T, in_smem);
+  return cudaGetLastError();
+}
+
+/* Threads the persistent kernel keeps resident on the device */
+uint64_t
+persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device)
+{
+  int nsm = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)block_size, 0);
+  if(blocks_per_sm) per_sm = std::min(per_sm, (int)blocks_per_sm);
+  return (uint64_t)std::max(per_sm, 1) * (uint64_t)nsm * block_size;
+}
+
+/* Device state of a set of items: tables, accumulators, counters */
+struct Plan {
+  int device = 0;
+  std::vector<DRequest> reqs;
+  std::vector<DScene> scenes;
+  std::vector<PItem> items;
+  std::vector<uint64_t> offsets;
+  std::vector<size_t> out_off;
+  DevBuf d_scenes, d_reqs, d_items, d_offsets, d_acc, d_cnt, d_out;
+  size_t acc_bytes = 0;
+  PTables T{};
+};
+
+static htrdr_gpu_res_T
+plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
+{
+  const int device = items[0].scene ? items[0].scene->device : -1;
+  for(size_t i = 0; i < n; ++i) {
+    if(!items[i].scene || items[i].scene->device != device || !items[i].buffer)
+      return HTRDR_GPU_RES_BAD_ARG;
+    const htrdr_gpu_buffer_layout& L = items[i].layout;
+    const htrdr_gpu_request& q = items[i].req;
+    if(L.width != q.width || L.height != q.height || L.elmt_size != pixel_size(q.mode)
+    || L.pitch < L.width * L.elmt_size)
+      return HTRDR_GPU_RES_BAD_ARG;
+  }
+  if(!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
+  P.device = device;
+  P.reqs.resize(n);
+  P.items.resize(n);
+  P.offsets.assign(n + 1, 0);
+  P.out_off.assign(n, 0);
+  std::vector<htrdr_gpu_scene*> scene_ptrs;
+  std::vector<uint64_t> acc_off(n);
+  uint64_t acc_total = 0;
+  size_t out_bytes = 0;
+  for(size_t i = 0; i < n; ++i) {
+    htrdr_gpu_res_T res = make_drequest(items[i].scene, &items[i].req, &P.reqs[i]);
+    if(res != HTRDR_GPU_RES_OK) return res;
+    auto it = std::find(scene_ptrs.begin(), scene_ptrs.end(), items[i].scene);
+    uint32_t si;
+    if(it == scene_ptrs.end()) {
+      si = (uint32_t)scene_ptrs.size();
+      scene_ptrs.push_back(items[i].scene);
+      P.scenes.push_back(items[i].scene->d);
+    } else {
+      si = (uint32_t)(it - scene_ptrs.begin());
+    }
+    const uint64_t npix = (uint64_t)P.reqs[i].width * P.reqs[i].height;
+    const uint32_t nch = P.reqs[i].mode == HG_IMAGE_CIE ? 3u : 1u;
+    acc_off[i] = acc_total;
+    acc_total += npix * (nch + 1);
+    P.items[i] = PItem{(uint32_t)i, si, 0};
+    P.offsets[i + 1] = P.offsets[i] + npix * P.reqs[i].nreal_pp;
+    P.out_off[i] = out_bytes;
+    if(host_out) out_bytes += (items[i].layout.pitch * items[i].layout.height + 255) & ~(size_t)255;
+  }
+  P.acc_bytes = acc_total * sizeof(DAccum);
+  if(!P.d_acc.alloc(P.acc_bytes) || !P.d_cnt.alloc(128) || !P.d_out.alloc(out_bytes))
+    return HTRDR_GPU_RES_MEM_ERR;
+  for(size_t i = 0; i < n; ++i) {
+    const uint64_t npix = (uint64_t)P.reqs[i].width * P.reqs[i].height;
+    const uint32_t nch = P.reqs[i].mode == HG_IMAGE_CIE ? 3u : 1u;
+    P.reqs[i].acc = (DAccum*)P.d_acc.ptr + acc_off[i];
+    P.reqs[i].tacc = P.reqs[i].acc + npix * nch;
+  }
+  if(!P.d_scenes.upload(P.scenes.data(), P.scenes.size() * sizeof(DScene))
+  || !P.d_reqs.upload(P.reqs.data(), n * sizeof(DRequest))
+  || !P.d_items.upload(P.items.data(), n * sizeof(PItem))
+  || !P.d_offsets.upload(P.offsets.data(), (n + 1) * 8))
+    return HTRDR_GPU_RES_MEM_ERR;
+  PTables& T = P.T;
+  T.scenes = (const DScene*)P.d_scenes.ptr;
+  T.reqs = (const DRequest*)P.d_reqs.ptr;
+  T.items = (const PItem*)P.d_items.ptr;
+  T.offsets = (const uint64_t*)P.d_offsets.ptr;
+  T.nscenes = (uint32_t)P.scenes.size();
+  T.nreqs = (uint32_t)n;
+  T.nitems = (uint32_t)n;
+  T.total = P.offsets[n];
+  T.cnt = P.d_cnt.ptr;
+  T.next = (unsigned long long*)((char*)P.d_cnt.ptr + 64);
+  return HTRDR_GPU_RES_OK;
+}
+
+/* Launch sequence of a plan: clear, persistent kernel, finalize into the
+ * items' output buffers (device) or the plan's staging (host copies after). */
+static bool
+plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning& tun,
+             bool host_out, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1, bool capturing = false)
+{
+  bool ok = cuda_ok(cudaMemsetAsync(P.d_acc.ptr, 0, P.acc_bytes, st), "memset")
+         && cuda_ok(cudaMemsetAsync(P.d_cnt.ptr, 0, 128, st), "memset");
+  PTables T = P.T;
+  T.chunk = tun.queue_chunk;
+  T.regroup_period = tun.regroup_period;
+  /* inside a stream capture an event record must be an external node to time
+   * the replays */
+  const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  if(ok && k0) ok = cuda_ok(cudaEventRecordWithFlags(k0, st, evf), "event");
+  if(ok) ok = cuda_ok(launch_persistent(T, tun.block_size, tun.blocks_per_sm, P.device, st), "k_persistent");
+  if(ok && k1) ok = cuda_ok(cudaEventRecordWithFlags(k1, st, evf), "event");
+  for(size_t i = 0; ok && i < n; ++i) {
+    char* dout = host_out ? (char*)P.d_out.ptr + P.out_off[i] : (char*)items[i].buffer;
+    ok = cuda_ok(launch_finalize(P.reqs[i], P.reqs[i].acc, P.reqs[i].tacc, dout,
+                                 items[i].layout.pitch, st), "k_finalize");
+    if(ok && host_out)
+      ok = cuda_ok(cudaMemcpyAsync(items[i].buffer, dout, items[i].layout.pitch * items[i].layout.height,
+                                   cudaMemcpyDeviceToHost, st), "D2H");
+  }
+  return ok;
+}
+
+static void
+read_stats(const unsigned long long c[5], float kms, float tms, htrdr_gpu_stats* stats)
+{
+  if(!stats) return;
+  stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
+  stats->realisations = c[3]; stats->failures = c[4];
+  stats->kernel_ms = kms; stats->total_ms = tms;
+}
 
 }  // namespace hg
 
@@ -194,118 +342,24 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
   htrdr_gpu_tuning tun;
   htrdr_gpu_default_tuning(&tun);
   if(tuning) tun = *tuning;
-  if(!tun.block_size || tun.block_size > 256 || (tun.block_size & 31) || !tun.queue_chunk)
-    return HTRDR_GPU_RES_BAD_ARG;
-  const int device = items[0].scene ? items[0].scene->device : -1;
-  for(size_t i = 0; i < n; ++i) {
-    if(!items[i].scene || items[i].scene->device != device || !items[i].buffer)
-      return HTRDR_GPU_RES_BAD_ARG;
-    const htrdr_gpu_buffer_layout& L = items[i].layout;
-    const htrdr_gpu_request& q = items[i].req;
-    if(L.width != q.width || L.height != q.height || L.elmt_size != pixel_size(q.mode)
-    || L.pitch < L.width * L.elmt_size)
-      return HTRDR_GPU_RES_BAD_ARG;
-  }
-  if(!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
-
-  std::vector<DRequest> reqs(n);
-  std::vector<uint32_t> req_scene(n);
-  std::vector<DScene> scenes;
-  std::vector<htrdr_gpu_scene*> scene_ptrs;
-  std::vector<uint64_t> offsets(n + 1, 0);
-  uint64_t acc_total = 0, tacc_total = 0;
-  size_t out_bytes = 0;
-  std::vector<size_t> out_off(n);
-  for(size_t i = 0; i < n; ++i) {
-    htrdr_gpu_res_T res = make_drequest(items[i].scene, &items[i].req, &reqs[i]);
-    if(res != HTRDR_GPU_RES_OK) return res;
-    auto it = std::find(scene_ptrs.begin(), scene_ptrs.end(), items[i].scene);
-    if(it == scene_ptrs.end()) {
-      req_scene[i] = (uint32_t)scene_ptrs.size();
-      scene_ptrs.push_back(items[i].scene);
-      scenes.push_back(items[i].scene->d);
-    } else {
-      req_scene[i] = (uint32_t)(it - scene_ptrs.begin());
-    }
-    const uint64_t npix = (uint64_t)reqs[i].width * reqs[i].height;
-    const uint32_t nch = reqs[i].mode == HG_IMAGE_CIE ? 3u : 1u;
-    reqs[i].acc_base = acc_total;
-    reqs[i].tacc_base = tacc_total;
-    acc_total += npix * nch;
-    tacc_total += npix;
-    offsets[i + 1] = offsets[i] + npix * reqs[i].nreal_pp;
-    out_off[i] = out_bytes;
-    if(host) out_bytes += (items[i].layout.pitch * items[i].layout.height + 255) & ~(size_t)255;
-  }
-  const uint64_t total = offsets[n];
-
-  DevBuf d_scenes, d_reqs, d_rs, d_off, d_acc, d_cnt, d_out;
-  const size_t acc_bytes = (acc_total + tacc_total) * sizeof(DAccum);
-  if(!d_scenes.upload(scenes.data(), scenes.size() * sizeof(DScene))
-  || !d_reqs.upload(reqs.data(), n * sizeof(DRequest))
-  || !d_rs.upload(req_scene.data(), n * 4)
-  || !d_off.upload(offsets.data(), (n + 1) * 8)
-  || !d_acc.alloc(acc_bytes) || !d_cnt.alloc(128) || !d_out.alloc(out_bytes))
-    return HTRDR_GPU_RES_MEM_ERR;
-
+  if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
+  Plan P;
+  htrdr_gpu_res_T res = plan_build(P, items, n, host);
+  if(res != HTRDR_GPU_RES_OK) return res;
   cudaStream_t st = items[0].scene->stream;
-  BatchTables B;
-  B.scenes = (const DScene*)d_scenes.ptr;
-  B.reqs = (const DRequest*)d_reqs.ptr;
-  B.req_scene = (const uint32_t*)d_rs.ptr;
-  B.offsets = (const uint64_t*)d_off.ptr;
-  B.nreq = (uint32_t)n;
-  B.total = total;
-  B.acc = (DAccum*)d_acc.ptr;
-  B.tacc = B.acc + acc_total;
-  B.cnt = (Counters*)d_cnt.ptr;
-  B.next = (unsigned long long*)((char*)d_cnt.ptr + 64);
-  B.chunk = tun.queue_chunk;
-  B.regroup_period = tun.regroup_period;
-
-  static_assert(sizeof(DScene) % 4 == 0 && sizeof(DRequest) % 4 == 0, "word copies");
-  const size_t tables = ((scenes.size() * sizeof(DScene) + 15) & ~(size_t)15) + n * sizeof(DRequest);
-  const int in_smem = tables <= 96 * 1024;
-  const size_t smem = in_smem ? tables : 0;
-  if(smem > 48 * 1024)
-    cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int nsm = 0, per_sm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)tun.block_size, smem);
-  if(tun.blocks_per_sm) per_sm = std::min(per_sm, (int)tun.blocks_per_sm);
-  per_sm = std::max(per_sm, 1);
-  const unsigned grid = (unsigned)(nsm * per_sm);
-
   cudaEvent_t e0, e1, e2, e3;
   cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
-  bool ok = true;
   cudaEventRecord(e0, st);
-  ok = ok && cuda_ok(cudaMemsetAsync(d_acc.ptr, 0, acc_bytes, st), "memset");
-  ok = ok && cuda_ok(cudaMemsetAsync(d_cnt.ptr, 0, 128, st), "memset");
-  cudaEventRecord(e1, st);
-  if(ok) {
-    k_persistent<<<grid, tun.block_size, smem, st>>>(B, (uint32_t)scenes.size(), in_smem);
-    ok = cuda_ok(cudaGetLastError(), "k_persistent");
-  }
-  cudaEventRecord(e2, st);
-  for(size_t i = 0; ok && i < n; ++i) {
-    char* dout = host ? (char*)d_out.ptr + out_off[i] : (char*)items[i].buffer;
-    ok = cuda_ok(launch_finalize(reqs[i], B.acc, B.tacc, dout, items[i].layout.pitch, st), "k_finalize");
-    if(ok && host)
-      ok = cuda_ok(cudaMemcpyAsync(items[i].buffer, dout, items[i].layout.pitch * items[i].layout.height,
-                                   cudaMemcpyDeviceToHost, st), "D2H");
-  }
+  bool ok = plan_enqueue(P, items, n, tun, host, st, e1, e2);
   cudaEventRecord(e3, st);
   unsigned long long c[5] = {0, 0, 0, 0, 0};
-  if(ok) ok = cuda_ok(cudaMemcpyAsync(c, d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H");
+  if(ok) ok = cuda_ok(cudaMemcpyAsync(c, P.d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H");
   if(ok) ok = cuda_ok(cudaStreamSynchronize(st), "sync");
-  if(ok && stats) {
+  if(ok) {
     float k = 0, t = 0;
     cudaEventElapsedTime(&k, e1, e2);
     cudaEventElapsedTime(&t, e0, e3);
-    stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
-    stats->realisations = c[3]; stats->failures = c[4];
-    stats->kernel_ms = k; stats->total_ms = t;
+    read_stats(c, k, t, stats);
   }
   cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   return ok ? HTRDR_GPU_RES_OK : HTRDR_GPU_RES_UNKNOWN_ERR;
@@ -353,5 +407,82 @@ htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best
         if(st.kernel_ms < best_t) { best_t = st.kernel_ms; *best = t; }
       }
   if(best_ms) *best_ms = best_t;
+  return HTRDR_GPU_RES_OK;
+}
+
+/*******************************************************************************
+ * Reusable batch: the whole launch sequence (clear, persistent kernel,
+ * finalize of every item) captured once in a CUDA graph and replayed.
+ ******************************************************************************/
+struct htrdr_gpu_batch {
+  Plan plan;
+  std::vector<htrdr_gpu_batch_item> items;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+};
+
+extern "C" HTRDR_GPU_API void
+htrdr_gpu_batch_release(htrdr_gpu_batch* b)
+{
+  if(!b) return;
+  cudaSetDevice(b->plan.device);
+  if(b->stream) cudaStreamSynchronize(b->stream);
+  if(b->exec) cudaGraphExecDestroy(b->exec);
+  if(b->graph) cudaGraphDestroy(b->graph);
+  if(b->e0) cudaEventDestroy(b->e0);
+  if(b->e1) cudaEventDestroy(b->e1);
+  if(b->e2) cudaEventDestroy(b->e2);
+  if(b->e3) cudaEventDestroy(b->e3);
+  if(b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_batch_create(const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuning,
+                       htrdr_gpu_batch** out)
+{
+  if(!items || !n || !out) return HTRDR_GPU_RES_BAD_ARG;
+  htrdr_gpu_tuning tun;
+  htrdr_gpu_default_tuning(&tun);
+  if(tuning) tun = *tuning;
+  if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
+  auto b = new htrdr_gpu_batch();
+  b->items.assign(items, items + n);
+  htrdr_gpu_res_T res = plan_build(b->plan, b->items.data(), n, false);
+  if(res != HTRDR_GPU_RES_OK) { htrdr_gpu_batch_release(b); return res; }
+  bool ok = cuda_ok(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream")
+         && cuda_ok(cudaEventCreate(&b->e0), "event") && cuda_ok(cudaEventCreate(&b->e1), "event")
+         && cuda_ok(cudaEventCreate(&b->e2), "event") && cuda_ok(cudaEventCreate(&b->e3), "event");
+  /* the occupancy query and the smem attribute are set outside the capture */
+  if(ok) ok = cuda_ok(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture");
+  if(ok) {
+    const bool enq = plan_enqueue(b->plan, b->items.data(), n, tun, false, b->stream, b->e1, b->e2, true);
+    ok = cuda_ok(cudaStreamEndCapture(b->stream, &b->graph), "end capture") && enq;
+  }
+  if(ok) ok = cuda_ok(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
+  if(!ok) { htrdr_gpu_batch_release(b); return HTRDR_GPU_RES_UNKNOWN_ERR; }
+  *out = b;
+  return HTRDR_GPU_RES_OK;
+}
+
+/* Replays the captured launch: the items' device buffers receive the maps. */
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_batch_run(htrdr_gpu_batch* b, htrdr_gpu_stats* stats)
+{
+  if(!b) return HTRDR_GPU_RES_BAD_ARG;
+  cudaSetDevice(b->plan.device);
+  unsigned long long c[5] = {0, 0, 0, 0, 0};
+  bool ok = cuda_ok(cudaEventRecord(b->e0, b->stream), "event")
+         && cuda_ok(cudaGraphLaunch(b->exec, b->stream), "graph launch")
+         && cuda_ok(cudaEventRecord(b->e3, b->stream), "event")
+         && cuda_ok(cudaMemcpyAsync(c, b->plan.d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, b->stream), "D2H")
+         && cuda_ok(cudaStreamSynchronize(b->stream), "sync");
+  if(!ok) return HTRDR_GPU_RES_UNKNOWN_ERR;
+  float k = 0, t = 0;
+  cudaEventElapsedTime(&k, b->e1, b->e2);
+  cudaEventElapsedTime(&t, b->e0, b->e3);
+  read_stats(c, k, t, stats);
   return HTRDR_GPU_RES_OK;
 }

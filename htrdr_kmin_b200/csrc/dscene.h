@@ -63,8 +63,8 @@ struct DRequest {
   int32_t mode;
   uint32_t width, height, spp, nreal_pp; /* nreal_pp = spp (x3 for CIE) */
   uint32_t seed;
-  uint64_t acc_base;     /* first channel accumulator of this request */
-  uint64_t tacc_base;    /* first time accumulator of this request */
+  struct DAccum* acc;    /* [npix][channels] FP64 accumulators of this request */
+  struct DAccum* tacc;   /* [npix] per-realisation time accumulators */
   double pix_sz[2];
   double wlen_range[2];  /* nm */
   /* wavelength sampler */

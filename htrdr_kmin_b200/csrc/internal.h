@@ -106,6 +106,30 @@ cudaError_t launch_sample_wavelength(const DRequest& R, int channel, size_t n, c
                                      const double* r1, uint32_t* cb, double* wlen, double* pdf,
                                      cudaStream_t st);
 
+/* Persistent engine (batched.cu).  A launch covers items, each a range of
+ * realisations [begin, begin + count) of one request; the realisations of
+ * all items form one work queue. */
+struct PItem {
+  uint32_t req;    /* index into reqs */
+  uint32_t scene;  /* index into scenes */
+  uint64_t begin;  /* first realisation (request index space) */
+};
+struct PTables {
+  const DScene* scenes;
+  const DRequest* reqs;   /* each with its own accumulators */
+  const PItem* items;
+  const uint64_t* offsets; /* [nitems+1] prefix sums of the items' counts */
+  uint32_t nscenes, nreqs, nitems;
+  uint64_t total;
+  unsigned long long* next; /* queue head (zeroed before the launch) */
+  void* cnt;                /* Counters (zeroed before the launch) */
+  uint32_t chunk, regroup_period;
+};
+cudaError_t launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
+                              int device, cudaStream_t st);
+bool valid_tuning(const htrdr_gpu_tuning& t);
+uint64_t persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device);
+
 }  // namespace hg
 
 #endif

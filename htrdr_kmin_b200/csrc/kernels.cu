@@ -25,13 +25,13 @@ accumulate(const Path& p, const DRequest& R, DAccum* acc, DAccum* tacc)
 {
   if(p.flags & PF_REJECTED) return;
   const uint32_t nch = R.mode == HG_IMAGE_CIE ? 3u : 1u;
-  DAccum* a = acc + R.acc_base + (size_t)p.pix * nch + p.chan;
+  DAccum* a = R.acc + (size_t)p.pix * nch + p.chan;
   if(p.flags & PF_FAILED) { atomicAdd(&a->pad, 1ull); return; }
   atomicAdd(&a->s, p.weight);
   atomicAdd(&a->s2, p.weight * p.weight);
   atomicAdd(&a->n, 1ull);
   const double us = (double)(gtimer() - p.t0) * 1e-3;
-  DAccum* t = tacc + R.tacc_base + p.pix;
+  DAccum* t = R.tacc + p.pix;
   atomicAdd(&t->s, us);
   atomicAdd(&t->s2, us * us);
   atomicAdd(&t->n, 1ull);
@@ -137,8 +137,8 @@ k_finalize(DRequest R, const DAccum* acc, const DAccum* tacc, char* out, size_t 
   const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
   if(pix >= R.width * R.height) return;
   const uint32_t x = pix % R.width, y = pix / R.width;
-  const DAccum t = tacc[R.tacc_base + pix];
-  const DAccum* ap = acc + R.acc_base;
+  const DAccum t = R.tacc[pix];
+  const DAccum* ap = R.acc;
   double* o = (double*)(out + (size_t)y * pitch + (size_t)x * (R.mode == HG_IMAGE_CIE ? 80 : 64));
   unsigned long long* ou = (unsigned long long*)o;
   if(R.mode == HG_FLUX_SW || R.mode == HG_FLUX_LW) {
@@ -253,7 +253,10 @@ launch_plain(const DScene& S, const DRequest& R, DAccum* acc, DAccum* tacc, uint
 {
   const uint64_t total = (uint64_t)npix * R.nreal_pp;
   if(!total) return cudaSuccess;
-  k_plain<<<nblocks(total, 128), 128, 0, st>>>(S, R, acc, tacc, pix_begin, npix, weights,
+  DRequest Ra = R;
+  Ra.acc = acc;
+  Ra.tacc = tacc;
+  k_plain<<<nblocks(total, 128), 128, 0, st>>>(S, Ra, acc, tacc, pix_begin, npix, weights,
                                                (Counters*)counters);
   return cudaGetLastError();
 }
@@ -263,7 +266,10 @@ launch_finalize(const DRequest& R, const DAccum* acc, const DAccum* tacc, void* 
                 cudaStream_t st)
 {
   const uint32_t npix = R.width * R.height;
-  k_finalize<<<nblocks(npix, 128), 128, 0, st>>>(R, acc, tacc, (char*)out, pitch);
+  DRequest Ra = R;
+  if(acc) Ra.acc = (DAccum*)acc;
+  if(tacc) Ra.tacc = (DAccum*)tacc;
+  k_finalize<<<nblocks(npix, 128), 128, 0, st>>>(Ra, acc, tacc, (char*)out, pitch);
   return cudaGetLastError();
 }
 

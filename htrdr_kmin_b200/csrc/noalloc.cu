@@ -189,8 +189,8 @@ htrdr_gpu_draw_map_noalloc(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   R.spp = req->spp;
   R.nreal_pp = req->spp * nch;
   R.seed = req->seed;
-  R.acc_base = 0;
-  R.tacc_base = npix * nch;
+  R.acc = sym.acc;
+  R.tacc = sym.acc + npix * nch;
   R.pix_sz[0] = 1.0 / (double)req->width;
   R.pix_sz[1] = 1.0 / (double)req->height;
   R.wlen_range[0] = r0;
@@ -228,7 +228,7 @@ htrdr_gpu_draw_map_noalloc(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   bool ok = cuda_ok(cudaMemsetAsync(sym.acc, 0, npix * (nch + 1) * sizeof(DAccum), st), "cudaMemsetAsync")
          && cuda_ok(cudaMemsetAsync(sym.cnt, 0, sizeof(g_noalloc_cnt), st), "cudaMemsetAsync");
   DAccum* acc = sym.acc;
-  DAccum* tacc = sym.acc;  /* tacc_base offsets the time accumulators */
+  DAccum* tacc = sym.acc + npix * nch;
   ok = ok && cuda_ok(launch_plain(scn->d, R, acc, tacc, 0, (uint32_t)npix, nullptr, sym.cnt, st), "k_plain");
   ok = ok && cuda_ok(launch_finalize(R, acc, tacc, device_buffer, layout->pitch, st), "k_finalize");
   ok = ok && cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");

@@ -383,8 +383,8 @@ make_drequest(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, DRequest* R)
   R->spp = req->spp;
   R->nreal_pp = req->spp * (req->mode == HG_IMAGE_CIE ? 3u : 1u);
   R->seed = req->seed;
-  R->acc_base = 0;
-  R->tacc_base = 0;
+  R->acc = nullptr;
+  R->tacc = nullptr;
   R->pix_sz[0] = 1.0 / (double)req->width;
   R->pix_sz[1] = 1.0 / (double)req->height;
   R->wlen_range[0] = req->wlen_range[0];

@@ -1,0 +1,442 @@
+/* Serving loop: continuous batching of draw_map requests.
+ *
+ * Client threads submit requests (scene, request, layout, host buffer) at any
+ * time.  One scheduling thread per server:
+ *   1. admits pending requests in arrival order while their device memory
+ *      (FP64 accumulators + output staging) fits in the HBM budget; the
+ *      accumulators stay resident until the request completes;
+ *   2. launches rounds of the persistent kernel, each over a share of the
+ *      not-yet-dispatched realisations of every admitted request; up to
+ *      `kDepth' rounds are in flight on their own streams, so the next round
+ *      fills the SMs that the slow paths of the previous one leave idle, and
+ *      the round size adapts to a target device time;
+ *   3. when a round ends, completes the requests whose realisations are all
+ *      accumulated (finalize kernel, copy of the map to the host buffer) and
+ *      frees their memory, which admits the next pending requests.
+ * Requests arriving while rounds run join the next round, so their work
+ * overlaps with the requests already on the GPU.  The weight of a realisation
+ * does not depend on how the work is split into rounds: a request gives the
+ * same map alone and in a mix (up to the FP64 summation order). */
+#include "internal.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+
+using namespace hg;
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+constexpr int kDepth = 3; /* rounds in flight */
+
+struct SReq {
+  uint64_t ticket = 0;
+  htrdr_gpu_scene* scene = nullptr;
+  htrdr_gpu_request req{};
+  htrdr_gpu_buffer_layout layout{};
+  void* host = nullptr;
+  DRequest dreq{};
+  DevBuf acc, out;
+  size_t acc_bytes = 0, out_bytes = 0;
+  uint64_t total = 0;      /* realisations of the request */
+  uint64_t next = 0;       /* first realisation not yet dispatched */
+  uint64_t completed = 0;  /* realisations of the rounds that ended */
+  int state = 0;           /* 0 pending, 1 active, 2 done */
+  htrdr_gpu_res_T result = HTRDR_GPU_RES_OK;
+  clk::time_point t_submit, t_done;
+};
+
+/* Device resources of one round in flight */
+struct Slot {
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  DevBuf scenes, reqs, items, offsets, cnt;
+  std::vector<std::pair<SReq*, uint64_t>> parts;
+  uint64_t seq = 0;
+  bool busy = false;
+};
+
+double
+ms_between(clk::time_point a, clk::time_point b)
+{
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+bool
+ensure(DevBuf& b, size_t bytes)
+{
+  if(b.ptr && b.bytes >= bytes) return true;
+  if(b.ptr) { cudaFree(b.ptr); b.ptr = nullptr; b.bytes = 0; }
+  return b.alloc(std::max<size_t>(bytes, 256));
+}
+
+}  // namespace
+
+struct htrdr_gpu_server {
+  htrdr_gpu_server_config cfg{};
+  std::thread worker;
+  std::mutex m;
+  std::condition_variable cv_work, cv_done;
+  bool stop = false;
+  std::deque<SReq*> pending;
+  std::vector<SReq*> active;
+  std::map<uint64_t, std::unique_ptr<SReq>> all;
+  uint64_t next_ticket = 1;
+  size_t hbm_used = 0, hbm_peak = 0;
+  uint64_t submitted = 0, completed = 0, failed = 0, rounds = 0, realisations = 0;
+  double busy_ms = 0;
+  std::vector<double> lat_ms;
+  clk::time_point t_first, t_last;
+  bool any = false;
+  cudaStream_t io = nullptr;
+  Slot slots[kDepth];
+  uint64_t seq = 0;
+  double round_real = 0;
+  double min_round = 0;   /* two waves of resident threads */
+  double rate = 0;        /* realisations/s, exponential average over rounds */
+  clk::time_point prev_done;
+  bool have_prev_done = false;
+
+  void finish(SReq* r, htrdr_gpu_res_T res)
+  { /* with m held */
+    r->result = res;
+    r->state = 2;
+    r->t_done = clk::now();
+    if(res == HTRDR_GPU_RES_OK) {
+      ++completed;
+      lat_ms.push_back(ms_between(r->t_submit, r->t_done));
+    } else {
+      ++failed;
+    }
+    t_last = r->t_done;
+    cv_done.notify_all();
+  }
+
+  void loop();
+  bool launch_round(Slot& s, const std::vector<SReq*>& act);
+};
+
+/* Fair share of the round budget over the requests with work left, then the
+ * leftovers in order; uploads the round's tables and launches it. */
+bool
+htrdr_gpu_server::launch_round(Slot& s, const std::vector<SReq*>& act)
+{
+  const uint64_t budget = (uint64_t)std::max(1.0, round_real);
+  std::vector<SReq*> todo;
+  for(SReq* r : act) if(r->next < r->total) todo.push_back(r);
+  if(todo.empty()) return true;
+  std::vector<uint64_t> counts(todo.size(), 0);
+  uint64_t left = budget;
+  const uint64_t share = std::max<uint64_t>(1, budget / todo.size());
+  for(size_t i = 0; i < todo.size(); ++i) {
+    counts[i] = std::min(todo[i]->total - todo[i]->next, std::min(share, left));
+    left -= counts[i];
+  }
+  for(size_t i = 0; i < todo.size() && left; ++i) {
+    const uint64_t c = std::min(todo[i]->total - todo[i]->next - counts[i], left);
+    counts[i] += c;
+    left -= c;
+  }
+  std::vector<DScene> scenes;
+  std::vector<htrdr_gpu_scene*> sp;
+  std::vector<DRequest> reqs;
+  std::vector<PItem> items;
+  std::vector<uint64_t> offsets(1, 0);
+  s.parts.clear();
+  for(size_t i = 0; i < todo.size(); ++i) {
+    if(!counts[i]) continue;
+    auto it = std::find(sp.begin(), sp.end(), todo[i]->scene);
+    uint32_t si;
+    if(it == sp.end()) { si = (uint32_t)sp.size(); sp.push_back(todo[i]->scene); scenes.push_back(todo[i]->scene->d); }
+    else si = (uint32_t)(it - sp.begin());
+    items.push_back(PItem{(uint32_t)reqs.size(), si, todo[i]->next});
+    reqs.push_back(todo[i]->dreq);
+    offsets.push_back(offsets.back() + counts[i]);
+    s.parts.emplace_back(todo[i], counts[i]);
+    todo[i]->next += counts[i];
+  }
+  if(!ensure(s.scenes, scenes.size() * sizeof(DScene)) || !ensure(s.reqs, reqs.size() * sizeof(DRequest))
+  || !ensure(s.items, items.size() * sizeof(PItem)) || !ensure(s.offsets, offsets.size() * 8)
+  || !ensure(s.cnt, 128))
+    return false;
+  bool ok = cuda_ok(cudaMemcpyAsync(s.scenes.ptr, scenes.data(), scenes.size() * sizeof(DScene),
+                                    cudaMemcpyHostToDevice, s.st), "H2D")
+         && cuda_ok(cudaMemcpyAsync(s.reqs.ptr, reqs.data(), reqs.size() * sizeof(DRequest),
+                                    cudaMemcpyHostToDevice, s.st), "H2D")
+         && cuda_ok(cudaMemcpyAsync(s.items.ptr, items.data(), items.size() * sizeof(PItem),
+                                    cudaMemcpyHostToDevice, s.st), "H2D")
+         && cuda_ok(cudaMemcpyAsync(s.offsets.ptr, offsets.data(), offsets.size() * 8,
+                                    cudaMemcpyHostToDevice, s.st), "H2D")
+         && cuda_ok(cudaMemsetAsync(s.cnt.ptr, 0, 128, s.st), "memset");
+  PTables T{};
+  T.scenes = (const DScene*)s.scenes.ptr;
+  T.reqs = (const DRequest*)s.reqs.ptr;
+  T.items = (const PItem*)s.items.ptr;
+  T.offsets = (const uint64_t*)s.offsets.ptr;
+  T.nscenes = (uint32_t)scenes.size();
+  T.nreqs = (uint32_t)reqs.size();
+  T.nitems = (uint32_t)items.size();
+  T.total = offsets.back();
+  T.cnt = s.cnt.ptr;
+  T.next = (unsigned long long*)((char*)s.cnt.ptr + 64);
+  T.chunk = cfg.tuning.queue_chunk;
+  T.regroup_period = cfg.tuning.regroup_period;
+  ok = ok && cuda_ok(cudaEventRecord(s.e0, s.st), "event")
+          && cuda_ok(launch_persistent(T, cfg.tuning.block_size, cfg.tuning.blocks_per_sm, cfg.device, s.st),
+                     "k_persistent")
+          && cuda_ok(cudaEventRecord(s.e1, s.st), "event");
+  realisations += T.total;
+  s.busy = true;
+  s.seq = seq++;
+  return ok;
+}
+
+void
+htrdr_gpu_server::loop()
+{
+  cudaSetDevice(cfg.device);
+  for(;;) {
+    std::unique_lock<std::mutex> lk(m);
+    /* admission by HBM budget, in arrival order */
+    while(!pending.empty()) {
+      SReq* r = pending.front();
+      const size_t need = r->acc_bytes + r->out_bytes;
+      if(need > cfg.hbm_budget_bytes) { pending.pop_front(); finish(r, HTRDR_GPU_RES_MEM_ERR); continue; }
+      if(hbm_used + need > cfg.hbm_budget_bytes) break;
+      pending.pop_front();
+      hbm_used += need;
+      hbm_peak = std::max(hbm_peak, hbm_used);
+      lk.unlock();
+      const bool ok = r->acc.alloc(r->acc_bytes) && r->out.alloc(r->out_bytes)
+                   && cuda_ok(cudaMemsetAsync(r->acc.ptr, 0, r->acc_bytes, io), "memset")
+                   && cuda_ok(cudaStreamSynchronize(io), "sync");
+      lk.lock();
+      if(!ok) { hbm_used -= need; finish(r, HTRDR_GPU_RES_MEM_ERR); continue; }
+      const uint32_t nch = r->dreq.mode == HG_IMAGE_CIE ? 3u : 1u;
+      r->dreq.acc = (DAccum*)r->acc.ptr;
+      r->dreq.tacc = r->dreq.acc + (uint64_t)r->dreq.width * r->dreq.height * nch;
+      r->state = 1;
+      active.push_back(r);
+    }
+    std::vector<SReq*> act = active;
+    lk.unlock();
+
+    /* keep up to kDepth rounds in flight */
+    bool launch_failed = false;
+    for(Slot& s : slots) {
+      if(s.busy) continue;
+      bool work = false;
+      for(SReq* r : act) work |= r->next < r->total;
+      if(!work) break;
+      if(!launch_round(s, act)) { launch_failed = true; break; }
+    }
+    Slot* oldest = nullptr;
+    for(Slot& s : slots) if(s.busy && (!oldest || s.seq < oldest->seq)) oldest = &s;
+
+    if(!oldest) {
+      lk.lock();
+      if(launch_failed) {
+        for(SReq* r : active) finish(r, HTRDR_GPU_RES_UNKNOWN_ERR);
+        active.clear();
+        continue;
+      }
+      if(stop && pending.empty() && active.empty()) break;
+      if(pending.empty()) cv_work.wait(lk);
+      continue;
+    }
+
+    /* wait for the oldest round, then complete the requests it finishes */
+    bool ok = cuda_ok(cudaEventSynchronize(oldest->e1), "round") && !launch_failed;
+    float ms = 0;
+    if(ok) cudaEventElapsedTime(&ms, oldest->e0, oldest->e1);
+    busy_ms += ms;
+    ++rounds;
+    { /* round size from the observed throughput (rounds overlap, so a
+       * round's own duration overstates its cost), at least two waves of
+       * the resident threads so that slow paths are amortised */
+      const clk::time_point now = clk::now();
+      uint64_t nreal = 0;
+      for(auto& pr : oldest->parts) nreal += pr.second;
+      if(have_prev_done) {
+        const double dt = std::max(1e-4, ms_between(prev_done, now) * 1e-3);
+        const double r = (double)nreal / dt;
+        rate = rate > 0 ? 0.7 * rate + 0.3 * r : r;
+        round_real = std::max(min_round, std::min(rate * cfg.round_target_ms * 1e-3, 1e12));
+      }
+      prev_done = now;
+      have_prev_done = true;
+    }
+    std::vector<SReq*> done;
+    for(auto& pr : oldest->parts) {
+      SReq* r = pr.first;
+      r->completed += pr.second;
+      if(!ok || r->completed < r->total) continue;
+      const bool fin = cuda_ok(launch_finalize(r->dreq, r->dreq.acc, r->dreq.tacc, r->out.ptr,
+                                               r->layout.pitch, oldest->st), "k_finalize")
+                    && cuda_ok(cudaMemcpyAsync(r->host, r->out.ptr, r->out_bytes, cudaMemcpyDeviceToHost,
+                                               oldest->st), "D2H")
+                    && cuda_ok(cudaStreamSynchronize(oldest->st), "sync");
+      if(!fin) r->result = HTRDR_GPU_RES_UNKNOWN_ERR;
+      done.push_back(r);
+    }
+    oldest->busy = false;
+    oldest->parts.clear();
+    lk.lock();
+    if(!ok) { /* a failed round poisons every active request */
+      for(Slot& s : slots) if(s.busy) { cudaStreamSynchronize(s.st); s.busy = false; s.parts.clear(); }
+      done = active;
+    }
+    for(SReq* r : done) {
+      if(r->state == 2) continue;
+      const size_t need = r->acc_bytes + r->out_bytes;
+      if(r->acc.ptr) { cudaFree(r->acc.ptr); r->acc.ptr = nullptr; }
+      if(r->out.ptr) { cudaFree(r->out.ptr); r->out.ptr = nullptr; }
+      hbm_used -= need;
+      active.erase(std::find(active.begin(), active.end(), r));
+      finish(r, ok ? r->result : HTRDR_GPU_RES_UNKNOWN_ERR);
+    }
+  }
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_create(const htrdr_gpu_server_config* cfg, htrdr_gpu_server** out)
+{
+  if(!cfg || !out || !cfg->hbm_budget_bytes || !valid_tuning(cfg->tuning)) return HTRDR_GPU_RES_BAD_ARG;
+  int ndev = 0;
+  if(cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+    set_error("no CUDA device available");
+    return HTRDR_GPU_RES_BAD_OP;
+  }
+  auto s = new htrdr_gpu_server();
+  s->cfg = *cfg;
+  if(s->cfg.round_target_ms <= 0) s->cfg.round_target_ms = 20.0;
+  cudaSetDevice(cfg->device);
+  /* smallest round: the configured first size, else two waves of resident threads */
+  s->min_round = cfg->round_realisations
+    ? (double)cfg->round_realisations
+    : 2.0 * (double)persistent_capacity(cfg->tuning.block_size, cfg->tuning.blocks_per_sm, cfg->device);
+  s->round_real = s->min_round;
+  bool ok = cuda_ok(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking), "stream");
+  for(Slot& sl : s->slots)
+    ok = ok && cuda_ok(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking), "stream")
+            && cuda_ok(cudaEventCreate(&sl.e0), "event") && cuda_ok(cudaEventCreate(&sl.e1), "event");
+  if(!ok) { htrdr_gpu_server_release(s); return HTRDR_GPU_RES_BAD_OP; }
+  s->worker = std::thread([s]() { s->loop(); });
+  *out = s;
+  return HTRDR_GPU_RES_OK;
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_submit(htrdr_gpu_server* s, htrdr_gpu_scene* scene, const htrdr_gpu_request* req,
+                        const htrdr_gpu_buffer_layout* layout, void* host_buffer, uint64_t* ticket)
+{
+  if(!s || !scene || !req || !layout || !host_buffer || !ticket) return HTRDR_GPU_RES_BAD_ARG;
+  if(scene->device != s->cfg.device) return HTRDR_GPU_RES_BAD_ARG;
+  if(layout->width != req->width || layout->height != req->height
+  || layout->elmt_size != pixel_size(req->mode) || layout->pitch < layout->width * layout->elmt_size)
+    return HTRDR_GPU_RES_BAD_ARG;
+  auto r = std::make_unique<SReq>();
+  cudaSetDevice(scene->device);
+  const htrdr_gpu_res_T res = make_drequest(scene, req, &r->dreq);
+  if(res != HTRDR_GPU_RES_OK) return res;
+  r->scene = scene;
+  r->req = *req;
+  r->layout = *layout;
+  r->host = host_buffer;
+  const uint64_t npix = (uint64_t)req->width * req->height;
+  const uint32_t nch = req->mode == HG_IMAGE_CIE ? 3u : 1u;
+  r->acc_bytes = npix * (nch + 1) * sizeof(DAccum);
+  r->out_bytes = layout->pitch * layout->height;
+  r->total = npix * r->dreq.nreal_pp;
+  r->t_submit = clk::now();
+  std::lock_guard<std::mutex> lk(s->m);
+  if(s->stop) return HTRDR_GPU_RES_BAD_OP;
+  r->ticket = s->next_ticket++;
+  *ticket = r->ticket;
+  if(!s->any) { s->any = true; s->t_first = r->t_submit; }
+  ++s->submitted;
+  s->pending.push_back(r.get());
+  s->all.emplace(r->ticket, std::move(r));
+  s->cv_work.notify_one();
+  return HTRDR_GPU_RES_OK;
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_poll(htrdr_gpu_server* s, uint64_t ticket, int* done, htrdr_gpu_res_T* result)
+{
+  if(!s || !done) return HTRDR_GPU_RES_BAD_ARG;
+  std::lock_guard<std::mutex> lk(s->m);
+  auto it = s->all.find(ticket);
+  if(it == s->all.end()) return HTRDR_GPU_RES_BAD_ARG;
+  *done = it->second->state == 2;
+  if(result) *result = it->second->result;
+  return HTRDR_GPU_RES_OK;
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_wait(htrdr_gpu_server* s, uint64_t ticket, double timeout_s, htrdr_gpu_res_T* result)
+{
+  if(!s) return HTRDR_GPU_RES_BAD_ARG;
+  std::unique_lock<std::mutex> lk(s->m);
+  auto it = s->all.find(ticket);
+  if(it == s->all.end()) return HTRDR_GPU_RES_BAD_ARG;
+  SReq* r = it->second.get();
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                      [r]() { return r->state == 2; });
+  if(!ok) return HTRDR_GPU_RES_BAD_OP;
+  if(result) *result = r->result;
+  return HTRDR_GPU_RES_OK;
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_stats(htrdr_gpu_server* s, struct htrdr_gpu_server_stats* st)
+{
+  if(!s || !st) return HTRDR_GPU_RES_BAD_ARG;
+  std::lock_guard<std::mutex> lk(s->m);
+  std::memset(st, 0, sizeof(*st));
+  st->submitted = s->submitted;
+  st->completed = s->completed;
+  st->failed = s->failed;
+  st->rounds = s->rounds;
+  st->realisations = s->realisations;
+  st->busy_ms = s->busy_ms;
+  st->hbm_peak_bytes = s->hbm_peak;
+  if(s->any && (s->completed || s->failed)) st->wall_ms = ms_between(s->t_first, s->t_last);
+  if(!s->lat_ms.empty()) {
+    std::vector<double> v = s->lat_ms;
+    std::sort(v.begin(), v.end());
+    auto q = [&](double f) { return v[std::min(v.size() - 1, (size_t)std::floor(f * (double)(v.size() - 1) + 0.5))]; };
+    st->p50_ms = q(0.50);
+    st->p99_ms = q(0.99);
+    st->max_ms = v.back();
+    double acc = 0;
+    for(double x : v) acc += x;
+    st->mean_ms = acc / (double)v.size();
+  }
+  return HTRDR_GPU_RES_OK;
+}
+
+extern "C" HTRDR_GPU_API void
+htrdr_gpu_server_release(htrdr_gpu_server* s)
+{
+  if(!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->m);
+    s->stop = true;
+    s->cv_work.notify_all();
+  }
+  if(s->worker.joinable()) s->worker.join();
+  cudaSetDevice(s->cfg.device);
+  for(Slot& sl : s->slots) {
+    if(sl.st) { cudaStreamSynchronize(sl.st); cudaStreamDestroy(sl.st); }
+    if(sl.e0) cudaEventDestroy(sl.e0);
+    if(sl.e1) cudaEventDestroy(sl.e1);
+  }
+  if(s->io) cudaStreamDestroy(s->io);
+  delete s;
+}

@@ -232,6 +232,59 @@ HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_autotune(struct htrdr_gpu_batch_item* items, size_t n, struct htrdr_gpu_tuning* best,
                    double* best_ms);
 
+/* Reusable batch (item buffers are device memory): the launch sequence is
+ * captured once in a CUDA graph; every run replays it. */
+struct htrdr_gpu_batch;
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_batch_create(const struct htrdr_gpu_batch_item* items, size_t n,
+                       const struct htrdr_gpu_tuning* tuning, struct htrdr_gpu_batch** batch);
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_batch_run(struct htrdr_gpu_batch* batch, struct htrdr_gpu_stats* stats);
+HTRDR_GPU_API void htrdr_gpu_batch_release(struct htrdr_gpu_batch* batch);
+
+/* ---- serving: a request loop with continuous batching ----
+ * Requests (scene, request, layout, host buffer) are submitted at any time.
+ * A scheduling thread admits them while their device memory (FP64
+ * accumulators + output staging) fits in the HBM budget, keeps their
+ * accumulators resident, and launches rounds of the persistent kernel over a
+ * share of every admitted request's remaining realisations; requests that
+ * arrive while a round runs join the next one.  A request completes when all
+ * its realisations are accumulated: its map is copied to its host buffer. */
+struct htrdr_gpu_server_config {
+  int device;
+  size_t hbm_budget_bytes;       /* admission budget for per-request device memory */
+  double round_target_ms;        /* rounds hold ~ this much work at the observed throughput */
+  uint64_t round_realisations;   /* smallest round (0: two waves of the kernel's resident threads) */
+  struct htrdr_gpu_tuning tuning;
+};
+struct htrdr_gpu_server_stats {
+  uint64_t submitted, completed, failed, rounds, realisations;
+  double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> map in the host buffer */
+  double busy_ms;                         /* device time of the rounds */
+  double wall_ms;                         /* first submit -> last completion */
+  size_t hbm_peak_bytes;
+};
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_create(const struct htrdr_gpu_server_config* config,
+                        struct htrdr_gpu_server** server);
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_submit(struct htrdr_gpu_server* server, struct htrdr_gpu_scene* scene,
+                        const struct htrdr_gpu_request* req,
+                        const struct htrdr_gpu_buffer_layout* layout, void* host_buffer,
+                        uint64_t* ticket);
+/* *done = 1 once the request's map is in its host buffer; *result its res_T */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_poll(struct htrdr_gpu_server* server, uint64_t ticket, int* done,
+                      htrdr_gpu_res_T* result);
+/* Blocks until the request completes (or timeout_s elapses: BAD_OP) */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_wait(struct htrdr_gpu_server* server, uint64_t ticket, double timeout_s,
+                      htrdr_gpu_res_T* result);
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_stats(struct htrdr_gpu_server* server, struct htrdr_gpu_server_stats* stats);
+/* Drains the submitted requests, then stops the scheduling thread */
+HTRDR_GPU_API void htrdr_gpu_server_release(struct htrdr_gpu_server* server);
+
 /* ---- library info ---- */
 HTRDR_GPU_API const char* htrdr_gpu_version(void);
 HTRDR_GPU_API int htrdr_gpu_device_count(void);

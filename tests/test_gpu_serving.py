@@ -1,0 +1,125 @@
+"""Serving loop (continuous batching) and graph-captured batches.
+
+A request gives the same map alone and in a mix served by the loop: every
+realisation has the same weight whatever the rounds it falls in, so per-pixel
+sums agree to the FP64 summation order (1e-9 relative)."""
+import random
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from htrdr_kmin_b200 import scene as S
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-9
+
+
+def _cmp(a, b, mode):
+    if mode in (S.MODE_FLUX_SW, S.MODE_FLUX_LW):
+        np.testing.assert_array_equal(a["n"], b["n"])
+        np.testing.assert_allclose(a["sum"], b["sum"], rtol=RTOL, atol=0)
+    elif mode == S.MODE_IMAGE_CIE:
+        for c in ("X", "Y", "Z"):
+            np.testing.assert_allclose(a[c], b[c], rtol=RTOL, atol=0)
+    else:
+        np.testing.assert_allclose(a["L"], b["L"], rtol=RTOL, atol=0)
+    np.testing.assert_array_equal(a["t_n"], b["t_n"])
+
+
+@pytest.fixture(scope="module")
+def mix(gpu_lib):
+    api = gpu_lib
+    s1, r1 = S.config_c1(scale=16 / 64, spp=16)
+    s2, r2 = S.config_c2(scale=32 / 128, spp=16, cloud_def=(16, 16, 8))
+    s3, r3 = S.config_c3(scale=12 / 512, spp=4, cloud_def=(32, 32, 8), nbands=6, nquad=3)
+    g1, g2, g3 = api.GpuScene(s1), api.GpuScene(s2, 0b100), api.GpuScene(s3)
+    reqs = [(g1, r1), (g2, r2), (g3, r3)]
+    rng = random.Random(4)
+    for i in range(9):
+        g, r = reqs[i % 3]
+        side = rng.choice([5, 8, 13, 20])
+        reqs.append((g, S.Request(**{**r.__dict__, "width": side, "height": side + 1,
+                                     "spp": rng.choice([2, 4, 8]), "seed": 100 + i})))
+    return reqs
+
+
+def test_server_results_equal_alone(gpu_lib, mix):
+    api = gpu_lib
+    alone = [gs.draw_map(r)[0] for gs, r in mix]
+    srv = api.Server(round_target_ms=2.0, round_realisations=4096)
+    tickets = [None] * len(mix)
+
+    def submitter(idx):
+        rng = random.Random(idx[0])
+        for i in idx:
+            time.sleep(rng.uniform(0, 0.01))
+            tickets[i] = srv.submit(*mix[i])
+
+    ts = [threading.Thread(target=submitter, args=(list(range(k, len(mix), 2)),)) for k in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    out = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(mix) and st["failed"] == 0
+    assert st["rounds"] > 1
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+    for (gs, r), a, b in zip(mix, out, alone):
+        _cmp(a, b, r.mode)
+
+
+def test_server_admission_by_budget(gpu_lib, mix):
+    api = gpu_lib
+    sizes = []
+    for gs, r in mix:
+        nch = 3 if r.mode == S.MODE_IMAGE_CIE else 1
+        sizes.append(r.width * r.height * (nch + 1) * 32 + r.width * r.height * r.pixel_size)
+    budget = max(sizes) + 16
+    srv = api.Server(hbm_budget_bytes=budget, round_target_ms=2.0, round_realisations=2048)
+    tickets = [srv.submit(gs, r) for gs, r in mix]
+    out = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert st["hbm_peak_bytes"] <= budget
+    for (gs, r), a in zip(mix, out):
+        _cmp(a, gs.draw_map(r)[0], r.mode)
+
+
+def test_server_rejects_request_above_budget(gpu_lib, mix):
+    api = gpu_lib
+    srv = api.Server(hbm_budget_bytes=1024)
+    t = srv.submit(*mix[0])
+    with pytest.raises(api.HtrdrError) as e:
+        srv.wait(t)
+    assert e.value.code == api.RES_MEM_ERR
+    srv.close()
+
+
+def test_graph_batch_replay(gpu_lib, mix):
+    import ctypes as C
+    import torch
+    api = gpu_lib
+    sub = mix[:4]
+    bufs = [torch.zeros(r.width * r.height * api.pixel_dtype(r.mode).itemsize, dtype=torch.uint8,
+                        device="cuda:0") for _, r in sub]
+    items = (api.BatchItem * len(sub))()
+    for i, (gs, r) in enumerate(sub):
+        items[i].scene = gs.handle.value
+        items[i].req = api.to_request(r)
+        items[i].layout = api.layout_for(r)
+        items[i].buffer = bufs[i].data_ptr()
+    h = C.c_void_p()
+    assert api.lib().htrdr_gpu_batch_create(items, len(sub), None, C.byref(h)) == 0
+    for _ in range(2):
+        st = api.Stats()
+        assert api.lib().htrdr_gpu_batch_run(h, C.byref(st)) == 0
+        assert st.kernel_ms > 0 and st.failures == 0
+        for (gs, r), b in zip(sub, bufs):
+            got = np.frombuffer(b.cpu().numpy().tobytes(), dtype=api.pixel_dtype(r.mode)).reshape(r.height, r.width)
+            _cmp(got, gs.draw_map(r)[0], r.mode)
+    api.lib().htrdr_gpu_batch_release(h)
