@@ -54,8 +54,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="lw_flux",
-                   choices=["lw_flux", "sw_image", "cie_image", "mix", "serve"])
+                   choices=["lw_flux", "sw_image", "cie_image", "cie_full", "mix", "serve"])
     p.add_argument("--rates", default="", help="serve: comma-separated arrival rates (requests/s)")
+    p.add_argument("--tuning", default="", help="block,chunk,period instead of the autotuner")
     p.add_argument("--cpu-sample-s", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -146,6 +147,10 @@ def workload(name: str):
         sc, rq = S.config_c3(scale=256 / 512, spp=16, cloud_def=(128, 128, 32))
         return [sc], [(0, rq)], ("CIE image 256x256 x 16 spp x 3 channels, 30 bands x 16 quad, cloud "
                                  "128x128x32 power-law (CIE config at 1/2 side, 1/4 spp, 1/8 cloud)")
+    if name == "cie_full":
+        sc, rq = S.config_c3()
+        return [sc], [(0, rq)], ("CIE image 512x512 x 64 spp x 3 channels, 30 bands x 16 quad, cloud "
+                                 "256x256x64 power-law of 50 m cells")
     scenes = S.batched_scenes(scale=0.25)
     reqs = S.batched_requests(n=24, side_range=(16, 96), spp_range=(16, 128))
     return scenes, reqs, ("24 uneven requests (side log-U[16,96], spp log-U[16,128], 50% SW / 50% LW "
@@ -373,7 +378,11 @@ def main():
             raise api.HtrdrError(what, res, L.htrdr_gpu_last_error().decode())
 
     # block size, queue chunk and regroup period from the autotuner (untimed)
-    tuning, _ = api.autotune(items_dev)
+    if args.tuning:
+        tuning = api.default_tuning()
+        tuning.block_size, tuning.queue_chunk, tuning.regroup_period = (int(x) for x in args.tuning.split(","))
+    else:
+        tuning, _ = api.autotune(items_dev)
 
     def step_batched():
         """all requests in one persistent launch, outputs left in HBM"""
@@ -473,7 +482,8 @@ def main():
             "config": {"workload": desc + ", batched persistent kernel",
                        "realisations_per_step_per_gpu": int(total_real),
                        "tuning": {"block_size": tuning.block_size, "queue_chunk": tuning.queue_chunk,
-                                  "regroup_period": tuning.regroup_period, "from": "autotuner"},
+                                  "regroup_period": tuning.regroup_period,
+                                  "from": "command line" if args.tuning else "autotuner"},
                        "l2": "inputs larger than L2: scenes of "
                              f"{sum(g.device_bytes for g in gss) / 1e6:.0f} MB resident",
                        "parallelism": ("replicated scene, independent streams per rank, NCCL sum of FP64 "

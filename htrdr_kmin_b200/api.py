@@ -66,7 +66,7 @@ class SceneDesc(C.Structure):
         ("has_ground", C.c_int32), ("ground_brdf", C.c_int32),
         ("ground_reflectivity", C.c_double), ("ground_temperature", C.c_double),
         ("sun_azimuth", C.c_double), ("sun_elevation", C.c_double),
-        ("props_mask", C.c_uint32),
+        ("props_mask", C.c_uint32), ("octree_on_host", C.c_int32),
     ]
 
 
@@ -233,7 +233,8 @@ def props_for_mode(mode: int) -> int:
 class GpuScene:
     """A scene resident in HBM with its majorant octrees (htsky_create)."""
 
-    def __init__(self, scene: S.Scene, props_mask: int = 0b111, device: int = 0):
+    def __init__(self, scene: S.Scene, props_mask: int = 0b111, device: int = 0,
+                 octree_on_host: bool = False):
         scene.validate()
         self.scene = scene
         keep: List[np.ndarray] = []
@@ -275,6 +276,7 @@ class GpuScene:
         d.sun_azimuth = scene.sun_azimuth
         d.sun_elevation = scene.sun_elevation
         d.props_mask = props_mask
+        d.octree_on_host = int(octree_on_host)
         h = C.c_void_p()
         _check(lib().htrdr_gpu_scene_create(device, C.byref(d), C.byref(h)), "htrdr_gpu_scene_create")
         self.handle = h

@@ -81,6 +81,14 @@ void build_octree(const DScene& hs, const float* lwc, const float* sig3, const f
                   uint32_t depth, uint32_t level_force, double tau, double cmax,
                   std::vector<uint32_t>& nodes);
 
+/* Octree build on the GPU (octree_gpu.cu), node arrays identical to build_octree */
+bool build_octrees_gpu(const DScene& S, const float* d_lwc, const int2* d_cl, const float* d_gka,
+                       const float* d_gks, const std::vector<float>& sig3,
+                       const std::vector<uint32_t>& band_of,
+                       const std::vector<std::pair<uint32_t, int>>& tasks, uint32_t level_force,
+                       double tau, double cmax, DevBuf& pool, std::vector<uint64_t>& base,
+                       std::vector<uint64_t>& count, cudaStream_t st);
+
 /* Kernel launchers (kernels.cu) */
 struct LaunchOut {
   unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;

@@ -605,38 +605,57 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
     for(uint32_t q = 0; q < nq; ++q)
       for(int p = 0; p < 3; ++p)
         if(desc->props_mask & (1u << p)) tasks.emplace_back(q, p);
-    std::vector<std::vector<uint32_t>> trees(tasks.size());
-    std::atomic<size_t> next(0);
-    const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for(unsigned t = 0; t < nth; ++t) {
-      pool.emplace_back([&]() {
-        for(;;) {
-          const size_t i = next++;
-          if(i >= tasks.size()) break;
-          const uint32_t q = tasks[i].first;
-          const int p = tasks[i].second;
-          build_octree(S, desc->cloud_lwc, &sig3[band_of[q] * 3], desc->gas_ka, desc->gas_ks,
-                       cl_lo.data(), cl_hi.data(), q, p, D, Lf, desc->optical_thickness, cmax,
-                       trees[i]);
-        }
-      });
+    if(desc->octree_on_host) { /* host build, in parallel over the trees */
+      std::vector<std::vector<uint32_t>> trees(tasks.size());
+      std::atomic<size_t> next(0);
+      const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+      std::vector<std::thread> pool;
+      for(unsigned t = 0; t < nth; ++t) {
+        pool.emplace_back([&]() {
+          for(;;) {
+            const size_t i = next++;
+            if(i >= tasks.size()) break;
+            const uint32_t q = tasks[i].first;
+            const int p = tasks[i].second;
+            build_octree(S, desc->cloud_lwc, &sig3[band_of[q] * 3], desc->gas_ka, desc->gas_ks,
+                         cl_lo.data(), cl_hi.data(), q, p, D, Lf, desc->optical_thickness, cmax,
+                         trees[i]);
+          }
+        });
+      }
+      for(auto& th : pool) th.join();
+      size_t total = 0;
+      for(size_t i = 0; i < tasks.size(); ++i) {
+        const size_t idx = (size_t)tasks[i].first * 3 + tasks[i].second;
+        scn->tree_base[idx] = total / 4;
+        scn->tree_count[idx] = trees[i].size() / 4;
+        total += trees[i].size();
+      }
+      std::vector<uint32_t> pool_nodes(total);
+      for(size_t i = 0; i < tasks.size(); ++i) {
+        const size_t idx = (size_t)tasks[i].first * 3 + tasks[i].second;
+        std::memcpy(&pool_nodes[scn->tree_base[idx] * 4], trees[i].data(), trees[i].size() * 4);
+      }
+      if(!(S.nodes = (const uint4*)upload(pool_nodes.data(), total * 4))) return HTRDR_GPU_RES_MEM_ERR;
+    } else { /* GPU build (octree_gpu.cu), same node arrays */
+      DevBuf d_ka, d_ks;
+      auto pool = std::make_unique<DevBuf>();
+      std::vector<uint64_t> base, count;
+      if(!d_ka.upload(desc->gas_ka, (size_t)nq * nl * 4) || !d_ks.upload(desc->gas_ks, (size_t)nq * nl * 4))
+        return HTRDR_GPU_RES_MEM_ERR;
+      if(!build_octrees_gpu(S, S.lwc, S.cell_layers, (const float*)d_ka.ptr, (const float*)d_ks.ptr, sig3,
+                            band_of, tasks, Lf, desc->optical_thickness, cmax, *pool, base, count, nullptr))
+        return HTRDR_GPU_RES_MEM_ERR;
+      for(size_t i = 0; i < tasks.size(); ++i) {
+        const size_t idx = (size_t)tasks[i].first * 3 + tasks[i].second;
+        scn->tree_base[idx] = base[i];
+        scn->tree_count[idx] = count[i];
+      }
+      S.nodes = (const uint4*)pool->ptr;
+      scn->bytes += pool->bytes;
+      scn->bufs.push_back(std::move(pool));
     }
-    for(auto& th : pool) th.join();
-    size_t total = 0;
-    for(size_t i = 0; i < tasks.size(); ++i) {
-      const size_t idx = (size_t)tasks[i].first * 3 + tasks[i].second;
-      scn->tree_base[idx] = total / 4;
-      scn->tree_count[idx] = trees[i].size() / 4;
-      total += trees[i].size();
-    }
-    std::vector<uint32_t> pool_nodes(total);
-    for(size_t i = 0; i < tasks.size(); ++i) {
-      const size_t idx = (size_t)tasks[i].first * 3 + tasks[i].second;
-      std::memcpy(&pool_nodes[scn->tree_base[idx] * 4], trees[i].data(), trees[i].size() * 4);
-    }
-    if(!(S.nodes = (const uint4*)upload(pool_nodes.data(), total * 4))
-    || !(S.tree_base = (const uint64_t*)upload(scn->tree_base.data(), scn->tree_base.size() * 8)))
+    if(!(S.tree_base = (const uint64_t*)upload(scn->tree_base.data(), scn->tree_base.size() * 8)))
       return HTRDR_GPU_RES_MEM_ERR;
   }
 

@@ -86,6 +86,7 @@ struct htrdr_gpu_scene_desc {
   double ground_temperature;    /* K */
   double sun_azimuth, sun_elevation; /* -D, degrees */
   uint32_t props_mask;          /* bit p: build the majorants of property p */
+  int32_t octree_on_host;       /* 1: build the octrees on the host CPU (else on the GPU) */
 };
 
 /* One run of the atmosphere command: sensor, spectral domain, output type

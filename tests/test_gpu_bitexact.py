@@ -40,6 +40,25 @@ def test_octrees_identical(gpu_lib, oracle_lib, name, scene, props):
                 assert np.all(g["kmin"] <= g["kmax"])
 
 
+def test_gpu_builder_matches_host_builder(gpu_lib):
+    """The GPU octree builder and the host builder emit the same node arrays
+    (and both match the oracle above) on a multi-band scene with -V and a
+    ragged grid."""
+    import time
+    scene, _ = S.config_c3(cloud_def=(96, 80, 24), nbands=5, nquad=4)
+    scene.grid_max_definition = (64, 0, 0)
+    t0 = time.time()
+    g = gpu_lib.GpuScene(scene)
+    t1 = time.time()
+    h = gpu_lib.GpuScene(scene, octree_on_host=True)
+    t2 = time.time()
+    print(f"octrees: GPU build {t1 - t0:.3f} s, host build {t2 - t1:.3f} s, {g.device_bytes / 1e6:.1f} MB")
+    for b in range(scene.nbands):
+        for q in range(int(scene.nquads[b])):
+            for p in range(3):
+                assert g.tree(b, q, p).tobytes() == h.tree(b, q, p).tobytes(), (b, q, p)
+
+
 def test_locate_leaf_identical(gpu_lib, oracle_lib):
     scene, _ = S.config_c3(cloud_def=(48, 40, 12), nbands=2, nquad=2)
     gs = gpu_lib.GpuScene(scene)
