@@ -10,8 +10,10 @@ seeded).  A step is one htrdr_draw_map of that map.
   HBM, scene (octrees) resident; device time from CUDA events recorded on the
   library's stream, max over ranks.
 * e2e: the same through the C ABI with a pinned host buffer
-  (htrdr_gpu_draw_map: request in, pixel buffer copied back), wall clock.
-* plain_gpu: the one-thread-per-realisation drop-in kernel on the same work.
+  (htrdr_gpu_draw_map on its default persistent engine with the same tuning;
+  request in, pixel buffer copied back), wall clock.
+* plain_gpu: the plain one-thread-per-realisation engine of the drop-in
+  (htrdr_gpu_draw_map_device with HTRDR_GPU_ENGINE_PLAIN) on the same work.
 * --impl reference: the CPU restatement of the reference path (oracle,
   OpenMP over all host cores) on a bounded sample of the same map.
 
@@ -54,7 +56,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="lw_flux",
-                   choices=["lw_flux", "sw_image", "cie_image", "cie_full", "mix", "serve"])
+                   choices=["lw_flux", "sw_image", "sw_large", "cie_image", "cie_full", "mix", "serve"])
     p.add_argument("--rates", default="", help="serve: comma-separated arrival rates (requests/s)")
     p.add_argument("--tuning", default="", help="block,chunk,period instead of the autotuner")
     p.add_argument("--cpu-sample-s", type=float, default=10.0)
@@ -143,6 +145,10 @@ def workload(name: str):
         sc, rq = S.config_c1()
         return [sc], [(0, rq)], ("SW image 64x64 x 32 spp, 1 band at 550 nm, 50 layers, cloud "
                                  "32x32x16 lognormal")
+    if name == "sw_large":
+        sc, rq = S.config_c1(scale=192 / 64)
+        return [sc], [(0, rq)], ("SW image 192x192 x 32 spp, 1 band at 550 nm, 50 layers, cloud "
+                                 "32x32x16 lognormal (SW config at 3x side: throughput-bound)")
     if name == "cie_image":
         sc, rq = S.config_c3(scale=256 / 512, spp=16, cloud_def=(128, 128, 32))
         return [sc], [(0, rq)], ("CIE image 256x256 x 16 spp x 3 channels, 30 bands x 16 quad, cloud "
@@ -230,7 +236,8 @@ def run_serve(args):
 
     For each rate the same arrival trace is served (a) by the request loop
     with continuous batching (htrdr_gpu_server_*) and (b) one request at a
-    time, in arrival order, by the plain drop-in kernel (htrdr_gpu_draw_map).
+    time, in arrival order, by the plain engine of the drop-in
+    (htrdr_gpu_draw_map with HTRDR_GPU_ENGINE_PLAIN).
     Latency = arrival -> map in the host buffer.  Throughput = realisations /
     (first arrival -> last completion)."""
     import threading
@@ -257,6 +264,8 @@ def run_serve(args):
         arr[i].scene, arr[i].req, arr[i].layout = gs.handle.value, api.to_request(r), api.layout_for(r)
         arr[i].buffer = dev[i].data_ptr()
     tuning, batched_ms = api.autotune(arr)
+    for g in gss:  # the one-at-a-time arm runs the plain engine of the drop-in
+        g.set_engine(api.ENGINE_PLAIN)
     plain_one = []
     for gs, r in items:
         _, st = gs.draw_map(r)
@@ -383,6 +392,8 @@ def main():
         tuning.block_size, tuning.queue_chunk, tuning.regroup_period = (int(x) for x in args.tuning.split(","))
     else:
         tuning, _ = api.autotune(items_dev)
+    for g in gss:  # the drop-in draw_map (e2e) runs the persistent engine with this tuning
+        g.set_engine(api.ENGINE_PERSISTENT, tuning)
 
     def step_batched():
         """all requests in one persistent launch, outputs left in HBM"""
@@ -392,13 +403,17 @@ def main():
         return st
 
     def step_plain():
-        """the plain drop-in kernel, one launch per request"""
+        """the plain engine of the drop-in, one launch per request"""
         k = 0.0
+        for isc, _ in reqs:
+            gss[isc].set_engine(api.ENGINE_PLAIN)
         for i, (isc, _) in enumerate(reqs):
             st = api.Stats()
             check(L.htrdr_gpu_draw_map_device(gss[isc].handle, C.byref(creq[i]), C.byref(clay[i]),
                                               C.c_void_p(dev[i].data_ptr()), C.byref(st)), "draw_map_device")
             k += st.kernel_ms
+        for isc, _ in reqs:
+            gss[isc].set_engine(api.ENGINE_PERSISTENT, tuning)
         return k
 
     def step_e2e():

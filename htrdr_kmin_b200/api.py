@@ -41,8 +41,10 @@ EXPORTED = [
     "htrdr_gpu_server_submit", "htrdr_gpu_server_poll", "htrdr_gpu_server_wait",
     "htrdr_gpu_server_stats", "htrdr_gpu_server_release",
     "htrdr_gpu_default_tuning", "htrdr_gpu_version", "htrdr_gpu_device_count",
-    "htrdr_gpu_last_error",
+    "htrdr_gpu_last_error", "htrdr_gpu_scene_set_engine", "htrdr_gpu_mode_tuning",
 ]
+
+ENGINE_PERSISTENT, ENGINE_PLAIN = 0, 1
 
 
 class HtrdrError(RuntimeError):
@@ -183,6 +185,9 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_server_release.restype = None
     L.htrdr_gpu_default_tuning.argtypes = [C.POINTER(Tuning)]
     L.htrdr_gpu_default_tuning.restype = None
+    L.htrdr_gpu_mode_tuning.argtypes = [i32, C.POINTER(Tuning)]
+    L.htrdr_gpu_mode_tuning.restype = None
+    L.htrdr_gpu_scene_set_engine.argtypes = [vp, i32, C.POINTER(Tuning)]
     L.htrdr_gpu_version.restype = C.c_char_p
     L.htrdr_gpu_last_error.restype = C.c_char_p
     L.htrdr_gpu_device_count.restype = C.c_int
@@ -308,6 +313,13 @@ class GpuScene:
                                                   n.value, C.byref(n)), "get_tree")
         return out
 
+    def set_engine(self, engine: int, tuning: Optional["Tuning"] = None):
+        """Engine of draw_map on this scene: ENGINE_PERSISTENT (default; tuning
+        None: by mode) or ENGINE_PLAIN."""
+        _check(lib().htrdr_gpu_scene_set_engine(self.handle, engine,
+                                                C.byref(tuning) if tuning is not None else None),
+               "htrdr_gpu_scene_set_engine")
+
     def draw_map(self, req: S.Request, device_out=None):
         """htrdr_draw_map: returns (pixel buffer [height, width], stats dict)."""
         r = to_request(req)
@@ -394,6 +406,12 @@ def default_tuning() -> Tuning:
     return t
 
 
+def mode_tuning(mode: int) -> Tuning:
+    t = Tuning()
+    lib().htrdr_gpu_mode_tuning(mode, C.byref(t))
+    return t
+
+
 def draw_maps_batched(items: Sequence[tuple], tuning: Optional[Tuning] = None):
     """Run many (GpuScene, Request) in one persistent kernel.  Returns the list
     of pixel buffers and the stats of the launch."""
@@ -408,8 +426,8 @@ def draw_maps_batched(items: Sequence[tuple], tuning: Optional[Tuning] = None):
         arr[i].layout = layout_for(req)
         arr[i].buffer = b.ctypes.data
     st = Stats()
-    t = tuning if tuning is not None else default_tuning()
-    _check(lib().htrdr_gpu_draw_maps_batched(arr, n, C.byref(t), C.byref(st)), "draw_maps_batched")
+    t = C.byref(tuning) if tuning is not None else None
+    _check(lib().htrdr_gpu_draw_maps_batched(arr, n, t, C.byref(st)), "draw_maps_batched")
     return bufs, st.as_dict()
 
 

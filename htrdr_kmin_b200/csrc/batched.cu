@@ -187,6 +187,49 @@ launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
   return cudaGetLastError();
 }
 
+struct SingleTables {
+  DScene scene;
+  DRequest req;
+  PItem item;
+  uint64_t offsets[2];
+};
+
+size_t
+single_tables_bytes()
+{
+  return sizeof(SingleTables);
+}
+
+cudaError_t
+launch_persistent_single(const DScene& S, const DRequest& R, void* tables, void* cnt,
+                         const htrdr_gpu_tuning& tun, int device, cudaStream_t st)
+{
+  SingleTables h;
+  h.scene = S;
+  h.req = R;
+  h.item = PItem{0, 0, 0};
+  h.offsets[0] = 0;
+  h.offsets[1] = (uint64_t)R.width * R.height * R.nreal_pp;
+  /* a pageable source is staged before the call returns: `h' may go */
+  cudaError_t e = cudaMemcpyAsync(tables, &h, sizeof(h), cudaMemcpyHostToDevice, st);
+  if(e != cudaSuccess) return e;
+  const SingleTables* d = (const SingleTables*)tables;
+  PTables T{};
+  T.scenes = &d->scene;
+  T.reqs = &d->req;
+  T.items = &d->item;
+  T.offsets = d->offsets;
+  T.nscenes = 1;
+  T.nreqs = 1;
+  T.nitems = 1;
+  T.total = h.offsets[1];
+  T.cnt = cnt;
+  T.next = (unsigned long long*)((char*)cnt + 64);
+  T.chunk = tun.queue_chunk;
+  T.regroup_period = tun.regroup_period;
+  return launch_persistent(T, tun.block_size, tun.blocks_per_sm, device, st);
+}
+
 /* Threads the persistent kernel keeps resident on the device */
 uint64_t
 persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device)
@@ -334,14 +377,42 @@ htrdr_gpu_default_tuning(htrdr_gpu_tuning* t)
   t->blocks_per_sm = 0;
 }
 
+/* Best of the autotuner's grid on the LW flux and SW/CIE image workloads */
+extern "C" HTRDR_GPU_API void
+htrdr_gpu_mode_tuning(int mode, htrdr_gpu_tuning* t)
+{
+  if(!t) return;
+  htrdr_gpu_default_tuning(t);
+  if(mode == HG_XWAVE_LW || mode == HG_FLUX_LW) {
+    t->block_size = 128;
+    t->queue_chunk = 1;
+    t->regroup_period = 1;
+  } else {
+    t->block_size = 256;
+    t->queue_chunk = 1;
+    t->regroup_period = 16;
+  }
+}
+
+/* `tuning' if given, else the default of the items' modes (SW/CIE if any) */
+static htrdr_gpu_tuning
+items_tuning(const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuning)
+{
+  htrdr_gpu_tuning tun;
+  if(tuning) return *tuning;
+  int sw = 0;
+  for(size_t i = 0; i < n; ++i)
+    sw |= items[i].req.mode != HG_XWAVE_LW && items[i].req.mode != HG_FLUX_LW;
+  htrdr_gpu_mode_tuning(sw ? HG_XWAVE_SW : HG_FLUX_LW, &tun);
+  return tun;
+}
+
 static htrdr_gpu_res_T
 batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuning,
              htrdr_gpu_stats* stats, bool host)
 {
   if(!items || !n) return HTRDR_GPU_RES_BAD_ARG;
-  htrdr_gpu_tuning tun;
-  htrdr_gpu_default_tuning(&tun);
-  if(tuning) tun = *tuning;
+  const htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
   if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
   Plan P;
   htrdr_gpu_res_T res = plan_build(P, items, n, host);
@@ -444,9 +515,7 @@ htrdr_gpu_batch_create(const htrdr_gpu_batch_item* items, size_t n, const htrdr_
                        htrdr_gpu_batch** out)
 {
   if(!items || !n || !out) return HTRDR_GPU_RES_BAD_ARG;
-  htrdr_gpu_tuning tun;
-  htrdr_gpu_default_tuning(&tun);
-  if(tuning) tun = *tuning;
+  const htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
   if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
   auto b = new htrdr_gpu_batch();
   b->items.assign(items, items + n);

@@ -1,4 +1,4 @@
-/* C ABI entry points of the plain drop-in path and of the checks. */
+/* C ABI entry points of the drop-in draw_map path (both engines) and of the checks. */
 #include "internal.h"
 
 #include <cmath>
@@ -9,7 +9,7 @@ using namespace hg;
 namespace {
 
 struct Workspace {
-  DevBuf acc, out, cnt;
+  DevBuf acc, out, cnt, tables;
   size_t acc_bytes = 0, out_bytes = 0;
 };
 
@@ -62,20 +62,32 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   const size_t acc_bytes = (size_t)npix * (nch + 1) * sizeof(DAccum);
   const size_t out_bytes = layout->pitch * layout->height;
   Workspace& ws = workspace(scn);
-  if(!ensure(ws.acc, acc_bytes) || !ensure(ws.cnt, 64)) return HTRDR_GPU_RES_MEM_ERR;
+  const bool plain = scn->engine == HTRDR_GPU_ENGINE_PLAIN;
+  if(!ensure(ws.acc, acc_bytes) || !ensure(ws.cnt, 128)) return HTRDR_GPU_RES_MEM_ERR;
+  if(!plain && !ensure(ws.tables, single_tables_bytes())) return HTRDR_GPU_RES_MEM_ERR;
   if(host && !ensure(ws.out, out_bytes)) return HTRDR_GPU_RES_MEM_ERR;
   DAccum* acc = (DAccum*)ws.acc.ptr;
   DAccum* tacc = acc + (size_t)npix * nch;
   void* dout = host ? ws.out.ptr : buffer;
+  htrdr_gpu_tuning tun;
+  if(scn->has_tuning) tun = scn->tuning;
+  else htrdr_gpu_mode_tuning(req->mode, &tun);
   cudaStream_t st = scn->stream;
   cudaEvent_t e0, e1, e2, e3;
   cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
   bool ok = true;
   cudaEventRecord(e0, st);
   ok = ok && cuda_ok(cudaMemsetAsync(acc, 0, acc_bytes, st), "cudaMemsetAsync");
-  ok = ok && cuda_ok(cudaMemsetAsync(ws.cnt.ptr, 0, 64, st), "cudaMemsetAsync");
+  ok = ok && cuda_ok(cudaMemsetAsync(ws.cnt.ptr, 0, 128, st), "cudaMemsetAsync");
   cudaEventRecord(e1, st);
-  ok = ok && cuda_ok(launch_plain(scn->d, R, acc, tacc, 0, npix, nullptr, ws.cnt.ptr, st), "k_plain");
+  if(plain) {
+    ok = ok && cuda_ok(launch_plain(scn->d, R, acc, tacc, 0, npix, nullptr, ws.cnt.ptr, st), "k_plain");
+  } else {
+    R.acc = acc;
+    R.tacc = tacc;
+    ok = ok && cuda_ok(launch_persistent_single(scn->d, R, ws.tables.ptr, ws.cnt.ptr, tun,
+                                                scn->device, st), "k_persistent");
+  }
   cudaEventRecord(e2, st);
   ok = ok && cuda_ok(launch_finalize(R, acc, tacc, dout, layout->pitch, st), "k_finalize");
   if(ok && host)
@@ -107,6 +119,19 @@ struct DevArr {
 };
 
 }  // namespace
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_scene_set_engine(htrdr_gpu_scene* scn, int engine, const htrdr_gpu_tuning* tuning)
+{
+  if(!scn) return HTRDR_GPU_RES_BAD_ARG;
+  if(engine != HTRDR_GPU_ENGINE_PERSISTENT && engine != HTRDR_GPU_ENGINE_PLAIN)
+    return HTRDR_GPU_RES_BAD_ARG;
+  if(tuning && !valid_tuning(*tuning)) return HTRDR_GPU_RES_BAD_ARG;
+  scn->engine = engine;
+  scn->has_tuning = tuning != nullptr;
+  if(tuning) scn->tuning = *tuning;
+  return HTRDR_GPU_RES_OK;
+}
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_map(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,

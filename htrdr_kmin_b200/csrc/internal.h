@@ -57,6 +57,11 @@ struct htrdr_gpu_scene {
   std::map<std::tuple<int, double, double, double>, std::unique_ptr<hg::Sampler>> samplers;
   std::mutex mtx;
   cudaStream_t stream = nullptr;
+  /* engine of draw_map on this scene (enum htrdr_gpu_engine) and the tuning
+   * of the persistent engine (has_tuning == 0: by mode) */
+  int engine = HTRDR_GPU_ENGINE_PERSISTENT;
+  int has_tuning = 0;
+  htrdr_gpu_tuning tuning{};
 };
 
 namespace hg {
@@ -137,6 +142,13 @@ cudaError_t launch_persistent(const PTables& T, uint32_t block_size, uint32_t bl
                               int device, cudaStream_t st);
 bool valid_tuning(const htrdr_gpu_tuning& t);
 uint64_t persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device);
+/* One request on the persistent engine.  `tables' (device memory of
+ * single_tables_bytes()) receives the launch's scene/request/item tables;
+ * `cnt' (device, 128 bytes) holds the counters and the queue head and must be
+ * zeroed before the launch. */
+size_t single_tables_bytes();
+cudaError_t launch_persistent_single(const DScene& S, const DRequest& R, void* tables, void* cnt,
+                                     const htrdr_gpu_tuning& tun, int device, cudaStream_t st);
 
 }  // namespace hg
 

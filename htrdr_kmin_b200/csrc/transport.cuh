@@ -38,9 +38,10 @@ namespace {
  * Word j of the stream (k0, k1, c0, c1) is word (j & 3) of
  * Philox4x32-10({c0, c1, j >> 2, 0}, {k0, k1}).
  ******************************************************************************/
-__device__ __forceinline__ void
-philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
-              uint32_t& o0, uint32_t& o1, uint32_t& o2, uint32_t& o3)
+/* Out of line: one copy of the ten rounds instead of one per draw site keeps
+ * the transport kernels inside the instruction cache. */
+__device__ __noinline__ uint4
+philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
 {
 #pragma unroll
   for(int r = 0; r < 10; ++r) {
@@ -53,7 +54,7 @@ philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, u
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
   }
-  o0 = c0; o1 = c1; o2 = c2; o3 = c3;
+  return make_uint4(c0, c1, c2, c3);
 }
 
 struct Rng {
@@ -67,7 +68,10 @@ struct Rng {
   __device__ __forceinline__ uint32_t u32()
   {
     const uint32_t i = n & 3u;
-    if(i == 0) philox4x32_10(c0, c1, n >> 2, 0u, k0, k1, b0, b1, b2, b3);
+    if(i == 0) {
+      const uint4 b = philox4x32_10(c0, c1, n >> 2, 0u, k0, k1);
+      b0 = b.x; b1 = b.y; b2 = b.z; b3 = b.w;
+    }
     ++n;
     return i == 0 ? b0 : (i == 1 ? b1 : (i == 2 ? b2 : b3));
   }
@@ -869,19 +873,31 @@ in_solar_cone(const DScene& S, float3 d)
 /*******************************************************************************
  * Events
  ******************************************************************************/
-/* Sensor sampling of realisation (pix, ireal): camera ray or flux probe,
- * wavelength, band and quadrature point (draw_map.c:51-107, 134-177,
- * 233-263, 348-384). */
-__device__ __forceinline__ void
-path_generate(Path& p, const DScene& S, const DRequest& R)
+struct GenOut {
+  Rng rng;               /* stream state after the sensor and spectral draws */
+  float3 org, rdir, dir; /* sensor ray; dir: direction of the first radiance call */
+  double wlen, inv_pdf;
+  uint32_t band, q, flags;
+  float cosN;
+  uint32_t chan;
+};
+
+/* The sampling part of path_generate, out of line (it runs once per
+ * realisation and is large: FP64 sensor and spectral sampling). */
+__device__ __noinline__ GenOut
+gen_sample(const DScene& S, const DRequest& R, uint32_t pix, uint32_t ireal)
 {
-  const uint32_t px = p.pix % R.width, py = p.pix / R.width;
-  p.rng.init(p.pix, R.seed, p.ireal, 0u);
+  GenOut g;
+  Path p; /* scratch holder so that the shared helpers below keep their form */
+  const uint32_t px = pix % R.width, py = pix / R.width;
+  p.rng.init(pix, R.seed, ireal, 0u);
   p.flags = 0;
-  p.w = 0.0;
-  p.c_seg = p.c_node = p.c_tc = 0;
-  p.t0 = gtimer();
-  p.chan = R.mode == HG_IMAGE_CIE ? (uint8_t)(p.ireal / R.spp) : 0;
+  p.chan = R.mode == HG_IMAGE_CIE ? (uint8_t)(ireal / R.spp) : 0;
+  g.chan = p.chan;
+  g.cosN = 0.f;
+  g.wlen = 0;
+  g.inv_pdf = 0;
+  g.band = g.q = 0;
   if(R.mode == HG_FLUX_SW || R.mode == HG_FLUX_LW) {
     const double s0 = ((double)px + p.rng.ud()) * R.pix_sz[0];
     const double s1 = ((double)py + p.rng.ud()) * R.pix_sz[1];
@@ -889,7 +905,10 @@ path_generate(Path& p, const DScene& S, const DRequest& R)
     for(int i = 0; i < 3; ++i)
       o[i] = R.rect_pos[i] + R.rect_ax[i] * (s0 * 2.0 - 1.0) + R.rect_ay[i] * (s1 * 2.0 - 1.0);
     p.org = mk3((float)o[0], (float)o[1], (float)o[2]);
-    if(S.has_ground && o[2] < 0) { p.flags |= PF_REJECTED; p.state = ST_DONE; return; }
+    if(S.has_ground && o[2] < 0) {
+      g.rng = p.rng; g.org = g.rdir = g.dir = p.org; g.flags = PF_REJECTED;
+      return g;
+    }
     const float u1 = p.rng.uf(), u2 = p.rng.uf();
     p.rdir = around(mk3((float)R.rect_n[0], (float)R.rect_n[1], (float)R.rect_n[2]),
                     sqrtf(1.f - u2), u1);
@@ -928,33 +947,126 @@ path_generate(Path& p, const DScene& S, const DRequest& R)
   const double wlen = sample_wavelength(R, p.chan, r0, r1, &pdf, &cb);
   pdf *= 1e9;
   const uint32_t band = find_band(S, wlen);
-  if(band >= S.nbands) { p.flags |= PF_REJECTED; p.state = ST_DONE; return; }
-  p.wlen = (float)wlen;
-  p.wlen_d = wlen;
-  p.band = band;
-  p.q = __ldg(S.quad_off + band) + sample_quad(S, r2, band);
-  p.inv_pdf = 1.0 / pdf;
-  p.pos = p.org;
-  p.dir = p.rdir;
+  g.org = p.org;
+  g.rdir = p.rdir;
+  g.dir = p.rdir;
+  if(band >= S.nbands) { g.rng = p.rng; g.flags = PF_REJECTED; return g; }
+  g.wlen = wlen;
+  g.band = band;
+  g.q = __ldg(S.quad_off + band) + sample_quad(S, r2, band);
+  g.inv_pdf = 1.0 / pdf;
+  g.flags = 0;
   switch(R.mode) {
-    case HG_XWAVE_LW: p.flags |= PF_LW; break;
-    case HG_FLUX_LW: p.flags |= PF_LW; p.inv_pdf = HG_PI_D / pdf; break;
+    case HG_XWAVE_LW: g.flags |= PF_LW; break;
+    case HG_FLUX_LW: g.flags |= PF_LW; g.inv_pdf = HG_PI_D / pdf; break;
     case HG_FLUX_SW: {
       const float3 sd = sun_sample(S, p.rng);
       const float3 nn = mk3((float)R.rect_n[0], (float)R.rect_n[1], (float)R.rect_n[2]);
-      p.cosN = dot3(nn, sd);
-      if(p.cosN <= 0.f) {
-        p.wdirect = 0.0;
-        p.flags |= PF_STAGE2 | PF_DIFFUSE;
+      g.cosN = dot3(nn, sd);
+      if(g.cosN <= 0.f) {
+        g.flags |= PF_STAGE2 | PF_DIFFUSE;
       } else {
-        p.dir = sd;
-        p.flags |= PF_DIRECT | PF_IN_CONE;
+        g.dir = sd;
+        g.flags |= PF_DIRECT | PF_IN_CONE;
       }
       break;
     }
-    default: p.flags |= PF_DIRECT | PF_DIFFUSE; break;
+    default: g.flags |= PF_DIRECT | PF_DIFFUSE; break;
   }
+  g.rng = p.rng;
+  return g;
+}
+
+/* Sensor sampling of realisation (pix, ireal): camera ray or flux probe,
+ * wavelength, band and quadrature point (draw_map.c:51-107, 134-177,
+ * 233-263, 348-384). */
+__device__ __forceinline__ void
+path_generate(Path& p, const DScene& S, const DRequest& R)
+{
+  const GenOut g = gen_sample(S, R, p.pix, p.ireal);
+  p.w = 0.0;
+  p.wdirect = 0.0;
+  p.c_seg = p.c_node = p.c_tc = 0;
+  p.t0 = gtimer();
+  p.rng = g.rng;
+  p.chan = (uint8_t)g.chan;
+  p.flags = g.flags;
+  p.org = g.org;
+  p.rdir = g.rdir;
+  if(g.flags & PF_REJECTED) { p.state = ST_DONE; return; }
+  p.wlen = (float)g.wlen;
+  p.wlen_d = g.wlen;
+  p.band = g.band;
+  p.q = g.q;
+  p.inv_pdf = g.inv_pdf;
+  p.cosN = g.cosN;
+  p.pos = g.org;
+  p.dir = g.dir;
   p.state = ST_RAD_BEGIN;
+}
+
+struct ScatOut {
+  Rng rng;
+  float3 dnext, sdir;
+  float R, refl, sun_ipdf;
+  uint32_t flags;
+};
+
+/* SW scattering event at the site of a collision with the scattering
+ * majorant (or at the ground): the next direction and the sun direction of
+ * the next-event estimate with its phase/BRDF value
+ * (htrdr_atmosphere_compute_radiance_sw.c:400-490).
+ * Out of line: it runs once per scattering and holds the FP64 sun sampling. */
+__device__ __noinline__ ScatOut
+sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float refl,
+           int site_cell, int site_layer, uint32_t band, uint32_t q)
+{
+  ScatOut o;
+  const float3 wo = neg3(dir);
+  const bool surface = (flags & PF_SURFACE) != 0;
+  float3 N = mk3(0.f, 0.f, 1.f);
+  bool specular = false;
+  o.refl = refl;
+  o.sdir = mk3(0.f, 0.f, 0.f);
+  if(surface) {
+    if(dot3(N, wo) < 0.f) N = neg3(N);
+    o.refl = S.ground_refl;
+    if(S.ground_brdf == 1) {
+      o.dnext = nrm3(add3(mul3(N, 2.f * dot3(N, wo)), neg3(wo)));
+      specular = true;
+    } else {
+      const float u1 = rng.uf(), u2 = rng.uf();
+      o.dnext = around(N, sqrtf(1.f - u2), u1);
+    }
+    flags &= ~PF_RAYLEIGH;
+  } else {
+    const double ks_gas = (double)site_k(S, site_cell, site_layer, band, q, HG_KS, 1);
+    const double ks_par = (double)site_k(S, site_cell, site_layer, band, q, HG_KS, 2);
+    const double ks = ks_par + ks_gas;
+    const bool ray = (double)rng.uf() < ks_gas / ks;
+    if(ray) flags |= PF_RAYLEIGH; else flags &= ~PF_RAYLEIGH;
+    const float u1 = rng.uf(), u2 = rng.uf();
+    o.dnext = around(dir, ray ? rayleigh_mu(u1) : hg_mu(g, u1), u2);
+  }
+  if(specular) flags |= PF_SPECULAR; else flags &= ~PF_SPECULAR;
+  if(surface && specular) {
+    if(!in_solar_cone(S, o.dnext)) o.R = 0.f;
+    else { o.sdir = o.dnext; o.R = dot3(N, o.sdir) < 0.f ? 0.f : o.refl; }
+    o.sun_ipdf = 1.f;
+  } else {
+    o.sdir = sun_sample(S, rng);
+    o.sun_ipdf = (float)S.sun_solid_angle;
+    if(surface) {
+      const float c = dot3(N, o.sdir);
+      o.R = c < 0.f ? 0.f : (S.ground_brdf == 1 ? 0.f : (c > 0.f ? o.refl / HG_PI_F : 0.f)) * c;
+    } else {
+      const float mu = dot3(dir, o.sdir);
+      o.R = (flags & PF_RAYLEIGH) ? rayleigh_eval(mu) : hg_eval(g, mu);
+    }
+  }
+  o.flags = flags;
+  o.rng = rng;
+  return o;
 }
 
 /* Advance the state machine until the path needs a voxel step (ST_TRACE),
@@ -1019,46 +1131,15 @@ path_event(Path& p, const DScene& S, const DRequest& R)
       case ST_SW_ABS_END: {
         p.tr_abs = p.tr.hit ? 0.f : (float)(p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
         if(p.tr_abs <= 0.f) { p.state = ST_RAD_END; break; }
-        const float3 wo = neg3(p.dir);
-        const bool surface = (p.flags & PF_SURFACE) != 0;
-        float3 N = mk3(0.f, 0.f, 1.f);
-        bool specular = false;
-        if(surface) {
-          if(dot3(N, wo) < 0.f) N = neg3(N);
-          p.refl = S.ground_refl;
-          if(S.ground_brdf == 1) {
-            p.dnext = nrm3(add3(mul3(N, 2.f * dot3(N, wo)), neg3(wo)));
-            specular = true;
-          } else {
-            const float u1 = p.rng.uf(), u2 = p.rng.uf();
-            p.dnext = around(N, sqrtf(1.f - u2), u1);
-          }
-          p.flags &= ~PF_RAYLEIGH;
-        } else {
-          const double ks_gas = (double)site_k(S, p.site_cell, p.site_layer, p.band, p.q, HG_KS, 1);
-          const double ks_par = (double)site_k(S, p.site_cell, p.site_layer, p.band, p.q, HG_KS, 2);
-          const double ks = ks_par + ks_gas;
-          const bool ray = (double)p.rng.uf() < ks_gas / ks;
-          if(ray) p.flags |= PF_RAYLEIGH; else p.flags &= ~PF_RAYLEIGH;
-          const float u1 = p.rng.uf(), u2 = p.rng.uf();
-          p.dnext = around(p.dir, ray ? rayleigh_mu(u1) : hg_mu(p.g, u1), u2);
-        }
-        if(specular) p.flags |= PF_SPECULAR; else p.flags &= ~PF_SPECULAR;
-        if(surface && specular) {
-          if(!in_solar_cone(S, p.dnext)) p.R = 0.f;
-          else { p.sdir = p.dnext; p.R = dot3(N, p.sdir) < 0.f ? 0.f : p.refl; }
-          p.sun_ipdf = 1.f;
-        } else {
-          p.sdir = sun_sample(S, p.rng);
-          p.sun_ipdf = (float)S.sun_solid_angle;
-          if(surface) {
-            const float c = dot3(N, p.sdir);
-            p.R = c < 0.f ? 0.f : (S.ground_brdf == 1 ? 0.f : (c > 0.f ? p.refl / HG_PI_F : 0.f)) * c;
-          } else {
-            const float mu = dot3(p.dir, p.sdir);
-            p.R = (p.flags & PF_RAYLEIGH) ? rayleigh_eval(mu) : hg_eval(p.g, mu);
-          }
-        }
+        const ScatOut so = sw_scatter(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
+                                      p.site_layer, p.band, p.q);
+        p.rng = so.rng;
+        p.flags = so.flags;
+        p.dnext = so.dnext;
+        p.sdir = so.sdir;
+        p.R = so.R;
+        p.refl = so.refl;
+        p.sun_ipdf = so.sun_ipdf;
         if(p.R > 0.f
         && ground_trace(S, p.pnext, p.sdir, 0.f, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0) < 0.f) {
           p.flags |= PF_TRACED;

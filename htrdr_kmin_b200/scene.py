@@ -194,7 +194,7 @@ def lwc_power_law(shape_zyx, seed: int, mean_gm3: float = 0.3, sigma: float = 0.
     k[0, 0, 0] = 1.0
     amp = k ** (-5.0 / 6.0)  # power ~ k^-5/3
     amp[0, 0, 0] = 0.0
-    g = np.fft.irfftn(f * amp, s=shape_zyx)
+    g = np.fft.irfftn(f * amp, s=shape_zyx, axes=(0, 1, 2))
     g = (g - g.mean()) / (g.std() + 1e-30)
     field_ = np.exp(sigma * g)
     field_ *= (mean_gm3 * 1e-3) / field_.mean()

@@ -137,10 +137,24 @@ htrdr_gpu_scene_get_tree(const struct htrdr_gpu_scene* scene, uint32_t iband, ui
                          int prop, void* nodes, size_t capacity, size_t* count);
 HTRDR_GPU_API uint32_t htrdr_gpu_scene_tree_depth(const struct htrdr_gpu_scene* scene);
 
-/* ---- plain drop-in driver: htrdr_draw_map(htrdr, args, buf) with the atmosphere
+/* ---- drop-in driver: htrdr_draw_map(htrdr, args, buf) with the atmosphere
  * callbacks (src/core/htrdr_draw_map.h:89-93, src/atmosphere/htrdr_atmosphere_draw_map.c:592-641).
  * Fills `buffer' (host memory, `layout') with atmosphere_pixel_{xwave,flux,image}
- * structs (src/atmosphere/htrdr_atmosphere_c.h:46-76). ---- */
+ * structs (src/atmosphere/htrdr_atmosphere_c.h:46-76).
+ *
+ * Two engines compute the same per-realisation weights (only the FP64
+ * summation order of a pixel differs): the persistent kernel with its work
+ * queue (default) and the plain one-thread-per-realisation kernel. ---- */
+enum htrdr_gpu_engine {
+  HTRDR_GPU_ENGINE_PERSISTENT = 0,
+  HTRDR_GPU_ENGINE_PLAIN = 1
+};
+struct htrdr_gpu_tuning;
+/* Engine of the scene's htrdr_gpu_draw_map(_device) calls; `tuning' (NULL: a
+ * default by mode) applies to the persistent engine. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_scene_set_engine(struct htrdr_gpu_scene* scene, int engine,
+                           const struct htrdr_gpu_tuning* tuning);
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_map(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
                    const struct htrdr_gpu_buffer_layout* layout, void* buffer,
@@ -216,7 +230,8 @@ struct htrdr_gpu_tuning {
   uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
 };
 /* Renders every item (each one htrdr_draw_map call of the reference) in one
- * persistent kernel; item buffers are host memory. */
+ * persistent kernel; item buffers are host memory.  tuning == NULL: the
+ * default of the items' modes (htrdr_gpu_mode_tuning; SW/CIE wins when mixed). */
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_maps_batched(struct htrdr_gpu_batch_item* items, size_t n,
                             const struct htrdr_gpu_tuning* tuning, struct htrdr_gpu_stats* stats);
@@ -226,6 +241,10 @@ htrdr_gpu_draw_maps_batched_device(struct htrdr_gpu_batch_item* items, size_t n,
                                    const struct htrdr_gpu_tuning* tuning,
                                    struct htrdr_gpu_stats* stats);
 HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
+/* Default tuning of a request mode: short LW paths want small blocks and
+ * regrouping at every step, long SW/CIE walks larger blocks and sparser
+ * regrouping. */
+HTRDR_GPU_API void htrdr_gpu_mode_tuning(int mode, struct htrdr_gpu_tuning* tuning);
 /* Autotuner: times the candidate tunings (block size, queue chunk, regroup
  * period) of the batched engine on `items' (device buffers) and returns the
  * fastest; the rendered values do not depend on the tuning. */

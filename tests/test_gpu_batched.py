@@ -46,8 +46,41 @@ def test_batched_equals_plain(gpu_lib):
     bufs, st = gpu_lib.draw_maps_batched(items)
     assert st["failures"] == 0
     for (gs, req), b in zip(items, bufs):
+        gs.set_engine(gpu_lib.ENGINE_PLAIN)
         p, _ = gs.draw_map(req)
+        gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
         _cmp(b, p, req.mode)
+
+
+def test_draw_map_engines_agree(gpu_lib):
+    """htrdr_gpu_draw_map on the persistent engine (default, by-mode or given
+    tuning) equals the plain engine, on host and device outputs."""
+    import torch
+    for gs, req in _mix(gpu_lib):
+        gs.set_engine(gpu_lib.ENGINE_PLAIN)
+        plain, sp = gs.draw_map(req)
+        gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
+        pers, spp = gs.draw_map(req)
+        _cmp(pers, plain, req.mode)
+        assert sp["realisations"] == spp["realisations"] and sp["segments"] == spp["segments"]
+        t = gpu_lib.default_tuning()
+        t.block_size, t.queue_chunk, t.regroup_period = 64, 2, 4
+        gs.set_engine(gpu_lib.ENGINE_PERSISTENT, t)
+        tuned, _ = gs.draw_map(req)
+        _cmp(tuned, plain, req.mode)
+        dev = torch.empty(pers.nbytes, dtype=torch.uint8, device="cuda:0")
+        gs.draw_map(req, device_out=dev.data_ptr())
+        torch.cuda.synchronize()
+        got = np.frombuffer(dev.cpu().numpy().tobytes(), dtype=pers.dtype).reshape(pers.shape)
+        _cmp(got, plain, req.mode)
+        gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
+    gs, req = _mix(gpu_lib)[0]
+    bad = gpu_lib.default_tuning()
+    bad.block_size = 48  # not a multiple of a warp
+    with pytest.raises(gpu_lib.HtrdrError):
+        gs.set_engine(gpu_lib.ENGINE_PERSISTENT, bad)
+    with pytest.raises(gpu_lib.HtrdrError):
+        gs.set_engine(7)
 
 
 def test_alone_equals_in_mix(gpu_lib):

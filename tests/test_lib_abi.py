@@ -57,3 +57,17 @@ def test_pixel_layouts_match_reference_structs():
     assert api.PIXEL_FLUX.itemsize == 64
     assert api.PIXEL_IMAGE.itemsize == 80
     assert C.sizeof(api.BufferLayout) == 40
+
+
+def test_engine_selection_and_mode_tuning_host_checks():
+    L = api.lib()
+    # a scene is required; unknown engines and invalid tunings are refused
+    assert L.htrdr_gpu_scene_set_engine(None, api.ENGINE_PLAIN, None) == api.RES_BAD_ARG
+    lw = api.mode_tuning(S.MODE_FLUX_LW)
+    sw = api.mode_tuning(S.MODE_XWAVE_SW)
+    cie = api.mode_tuning(S.MODE_IMAGE_CIE)
+    for t in (lw, sw, cie):
+        assert t.block_size % 32 == 0 and 0 < t.block_size <= 512 and t.queue_chunk >= 1
+    assert (lw.block_size, lw.regroup_period) != (sw.block_size, sw.regroup_period)
+    assert (sw.block_size, sw.queue_chunk, sw.regroup_period) == \
+        (cie.block_size, cie.queue_chunk, cie.regroup_period)
