@@ -20,7 +20,7 @@ seeded).  A step is one htrdr_draw_map of that map.
 Other workloads (development and profiling): ``sw_image`` (SW image 64x64 x 32
 spp, one band at 550 nm, 32x32x16 cloud), ``cie_image`` (CIE image 256x256 x
 16 spp x 3 channels, 30 bands x 16 points, 128x128x32 power-law cloud) and
-``mix`` (24 uneven SW/LW image requests on three scenes in one launch, against
+``mix`` (64 uneven SW/LW image requests on three scenes in one launch, against
 the same requests one at a time on the plain kernel).
 
 Multi-GPU (torchrun): every rank renders the whole map with its own random
@@ -158,8 +158,8 @@ def workload(name: str):
         return [sc], [(0, rq)], ("CIE image 512x512 x 64 spp x 3 channels, 30 bands x 16 quad, cloud "
                                  "256x256x64 power-law of 50 m cells")
     scenes = S.batched_scenes(scale=0.25)
-    reqs = S.batched_requests(n=24, side_range=(16, 96), spp_range=(16, 128))
-    return scenes, reqs, ("24 uneven requests (side log-U[16,96], spp log-U[16,128], 50% SW / 50% LW "
+    reqs = S.batched_requests(n=64, side_range=(16, 96), spp_range=(16, 128))
+    return scenes, reqs, ("64 uneven requests (side log-U[16,96], spp log-U[16,128], 50% SW / 50% LW "
                           "images) on 3 cloud scenes (32^3, 64x64x16, 128x128x32) in one launch")
 
 
@@ -273,7 +273,8 @@ def run_serve(args):
     rates = [float(x) for x in args.rates.split(",")] if args.rates else None
     if not rates:
         capacity = len(items) / (sum(plain_one) * 1e-3)  # plain, one at a time, requests/s
-        rates = [0.5 * capacity, 1.0 * capacity, 2.0 * capacity, 4.0 * capacity]
+        # from below the plain path's capacity to well above the batched engine's
+        rates = [f * capacity for f in (0.5, 1.0, 2.0, 4.0, 8.0, 16.0)]
     rng = np.random.default_rng(5)
     sweep = []
     for rate in rates:
