@@ -58,10 +58,39 @@ def parse():
     p.add_argument("--workload", default="lw_flux",
                    choices=["lw_flux", "sw_image", "sw_large", "cie_image", "cie_full", "mix", "serve"])
     p.add_argument("--rates", default="", help="serve: comma-separated arrival rates (requests/s)")
-    p.add_argument("--tuning", default="", help="block,chunk,period instead of the autotuner")
+    p.add_argument("--tuning", default="",
+                   help="block,chunk,period[,engine[,budget[,slots[,tail]]]] instead of the autotuner "
+                        "(engine 0 persistent, 2 wavefront)")
     p.add_argument("--cpu-sample-s", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
+
+
+def parse_tuning(api, text: str):
+    """block,chunk,period[,engine[,budget[,slots[,tail]]]] -> Tuning"""
+    t = api.default_tuning()
+    v = [int(x) for x in text.split(",")]
+    t.block_size, t.queue_chunk, t.regroup_period = v[:3]
+    if len(v) > 3:
+        t.engine = v[3]
+    if len(v) > 4:
+        t.trace_budget = v[4]
+    if len(v) > 5:
+        t.wave_slots = v[5]
+    if len(v) > 6:
+        t.wave_tail = v[6]
+    return t
+
+
+def tuning_dict(t, source: str) -> dict:
+    d = {"engine": {0: "persistent", 2: "wavefront"}.get(t.engine, str(t.engine)),
+         "block_size": t.block_size}
+    if t.engine == 2:
+        d.update(trace_budget=t.trace_budget or 256, wave_slots=t.wave_slots or "auto")
+    else:
+        d.update(queue_chunk=t.queue_chunk, regroup_period=t.regroup_period)
+    d["from"] = source
+    return d
 
 
 def dist_env():
@@ -264,6 +293,9 @@ def run_serve(args):
         arr[i].scene, arr[i].req, arr[i].layout = gs.handle.value, api.to_request(r), api.layout_for(r)
         arr[i].buffer = dev[i].data_ptr()
     tuning, batched_ms = api.autotune(arr)
+    if tuning.engine != api.ENGINE_PERSISTENT:  # the server's rounds run the persistent engine
+        tuning = api.mode_tuning(S.MODE_XWAVE_SW)
+        tuning.engine = api.ENGINE_PERSISTENT
     for g in gss:  # the one-at-a-time arm runs the plain engine of the drop-in
         g.set_engine(api.ENGINE_PLAIN)
     plain_one = []
@@ -327,9 +359,7 @@ def run_serve(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scenes and sensors), Poisson arrivals",
             "config": {"workload": "serving: " + desc, "rates_req_s": rates,
-                       "hbm_budget_GB": 150, "tuning": {"block_size": tuning.block_size,
-                                                        "queue_chunk": tuning.queue_chunk,
-                                                        "regroup_period": tuning.regroup_period}},
+                       "hbm_budget_GB": 150, "tuning": tuning_dict(tuning, "autotuner / mode default")},
             "serving": sweep,
             "batched_one_launch_Mreal_s": total_real / (batched_ms * 1e-3) / 1e6,
             "plain_sequential_Mreal_s": total_real / (sum(plain_one) * 1e-3) / 1e6,
@@ -387,17 +417,17 @@ def main():
         if res != 0:
             raise api.HtrdrError(what, res, L.htrdr_gpu_last_error().decode())
 
-    # block size, queue chunk and regroup period from the autotuner (untimed)
+    # engine, block size, queue chunk, regroup period, step budget from the
+    # autotuner (untimed)
     if args.tuning:
-        tuning = api.default_tuning()
-        tuning.block_size, tuning.queue_chunk, tuning.regroup_period = (int(x) for x in args.tuning.split(","))
+        tuning = parse_tuning(api, args.tuning)
     else:
         tuning, _ = api.autotune(items_dev)
-    for g in gss:  # the drop-in draw_map (e2e) runs the persistent engine with this tuning
-        g.set_engine(api.ENGINE_PERSISTENT, tuning)
+    for g in gss:  # the drop-in draw_map (e2e) runs the same engine and tuning
+        g.set_engine(tuning.engine, tuning)
 
     def step_batched():
-        """all requests in one persistent launch, outputs left in HBM"""
+        """all requests in one launch of the work-queue engine, outputs left in HBM"""
         st = api.Stats()
         check(L.htrdr_gpu_draw_maps_batched_device(items_dev, n, C.byref(tuning), C.byref(st)),
               "batched_device")
@@ -414,7 +444,7 @@ def main():
                                               C.c_void_p(dev[i].data_ptr()), C.byref(st)), "draw_map_device")
             k += st.kernel_ms
         for isc, _ in reqs:
-            gss[isc].set_engine(api.ENGINE_PERSISTENT, tuning)
+            gss[isc].set_engine(tuning.engine, tuning)
         return k
 
     def step_e2e():
@@ -480,6 +510,7 @@ def main():
         step_ms, e2e_ms = float(t[0]), float(t[1])
 
     last = stats[-1]
+    wave = tuning.engine == api.ENGINE_WAVEFRONT
     reals = last.realisations
     value = world * reals / (step_ms * 1e-3) / 1e6
     kms = float(np.mean(kernel_ms))
@@ -495,11 +526,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scenes and sensors)",
-            "config": {"workload": desc + ", batched persistent kernel",
+            "config": {"workload": desc + (", wavefront engine" if wave else ", batched persistent kernel"),
                        "realisations_per_step_per_gpu": int(total_real),
-                       "tuning": {"block_size": tuning.block_size, "queue_chunk": tuning.queue_chunk,
-                                  "regroup_period": tuning.regroup_period,
-                                  "from": "command line" if args.tuning else "autotuner"},
+                       "tuning": tuning_dict(tuning, "command line" if args.tuning else "autotuner"),
                        "l2": "inputs larger than L2: scenes of "
                              f"{sum(g.device_bytes for g in gss) / 1e6:.0f} MB resident",
                        "parallelism": ("replicated scene, independent streams per rank, NCCL sum of FP64 "
@@ -508,11 +537,11 @@ def main():
             "e2e": {"value": world * reals / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
                     "h2d_bytes_per_step": int(n * (C.sizeof(api.Request) + C.sizeof(api.BufferLayout))),
                     "d2h_bytes_per_step": int(out_bytes)},
-            "gpu_launches": (1 + n) * args.steps,
+            "gpu_launches": int(sum(s.launches for s in stats)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "k_persistent", "alg_bytes_per_launch": int(alg_bytes),
-                         "kernel_ms": kms},
+                         "kernel": "k_wave_event + k_wave_trace" if wave else "k_persistent",
+                         "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": kms},
             "cpu_baseline": cpu,
             "plain_gpu": {"value": reals / (plain_ms * 1e-3) / 1e6, "unit": UNIT, "kernel": "k_plain",
                           "kernel_ms": plain_ms, "launches": n},

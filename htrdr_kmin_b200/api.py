@@ -44,7 +44,7 @@ EXPORTED = [
     "htrdr_gpu_last_error", "htrdr_gpu_scene_set_engine", "htrdr_gpu_mode_tuning",
 ]
 
-ENGINE_PERSISTENT, ENGINE_PLAIN = 0, 1
+ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT = 0, 1, 2
 
 
 class HtrdrError(RuntimeError):
@@ -92,7 +92,7 @@ class BufferLayout(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("realisations", C.c_uint64), ("segments", C.c_uint64), ("nodes", C.c_uint64),
                 ("collisions", C.c_uint64), ("failures", C.c_uint64),
-                ("kernel_ms", C.c_double), ("total_ms", C.c_double)]
+                ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("launches", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -100,7 +100,12 @@ class Stats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("block_size", C.c_uint32), ("queue_chunk", C.c_uint32),
-                ("regroup_period", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+                ("regroup_period", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("engine", C.c_uint32), ("wave_slots", C.c_uint32),
+                ("trace_budget", C.c_uint32), ("wave_tail", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
 class BatchItem(C.Structure):
@@ -314,8 +319,9 @@ class GpuScene:
         return out
 
     def set_engine(self, engine: int, tuning: Optional["Tuning"] = None):
-        """Engine of draw_map on this scene: ENGINE_PERSISTENT (default; tuning
-        None: by mode) or ENGINE_PLAIN."""
+        """Engine of draw_map on this scene: ENGINE_PERSISTENT, ENGINE_WAVEFRONT
+        (tuning None: the mode's) or ENGINE_PLAIN.  Without a call, the
+        mode's default tuning decides, engine included."""
         _check(lib().htrdr_gpu_scene_set_engine(self.handle, engine,
                                                 C.byref(tuning) if tuning is not None else None),
                "htrdr_gpu_scene_set_engine")

@@ -19,42 +19,15 @@
  *
  * Entry points: one-shot htrdr_gpu_draw_maps_batched(_device), the reusable
  * htrdr_gpu_batch_* object whose launch sequence is captured once in a CUDA
- * graph and replayed, and the autotuner. */
-#include "internal.h"
-#include "transport.cuh"
+ * graph and replayed, and the autotuner.  The one-shot entry points and the
+ * autotuner also run the same items on the wavefront engine (wavefront.cu)
+ * when the tuning selects it. */
+#include "engine.cuh"
 
 #include <algorithm>
 #include <cstring>
 
 namespace hg {
-
-__device__ __forceinline__ uint32_t
-find_item(const PTables& T, uint64_t g)
-{
-  uint32_t lo = 0, hi = T.nitems; /* last item whose offset <= g */
-  while(hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if(__ldg(T.offsets + mid) <= g) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ void
-accumulate_b(const Path& p, const DRequest& R)
-{
-  if(p.flags & PF_REJECTED) return;
-  const uint32_t nch = R.mode == HG_IMAGE_CIE ? 3u : 1u;
-  DAccum* a = R.acc + (size_t)p.pix * nch + p.chan;
-  if(p.flags & PF_FAILED) { atomicAdd(&a->pad, 1ull); return; }
-  atomicAdd(&a->s, p.weight);
-  atomicAdd(&a->s2, p.weight * p.weight);
-  atomicAdd(&a->n, 1ull);
-  const double us = (double)(gtimer() - p.t0) * 1e-3;
-  DAccum* t = R.tacc + p.pix;
-  atomicAdd(&t->s, us);
-  atomicAdd(&t->s2, us * us);
-  atomicAdd(&t->n, 1ull);
-}
 
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
 k_persistent(PTables T, int tables_in_smem)
@@ -62,23 +35,13 @@ k_persistent(PTables T, int tables_in_smem)
   /* the scene and request views are read on every step: keep them in shared
    * memory when they fit (one copy per block) */
   extern __shared__ __align__(16) unsigned char smem[];
-  if(tables_in_smem) {
-    DScene* ss = (DScene*)smem;
-    DRequest* sr = (DRequest*)(smem + ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15));
-    const uint32_t* gs = (const uint32_t*)T.scenes;
-    const uint32_t* gr = (const uint32_t*)T.reqs;
-    for(uint32_t i = threadIdx.x; i < T.nscenes * sizeof(DScene) / 4; i += blockDim.x) ((uint32_t*)ss)[i] = gs[i];
-    for(uint32_t i = threadIdx.x; i < T.nreqs * sizeof(DRequest) / 4; i += blockDim.x) ((uint32_t*)sr)[i] = gr[i];
-    __syncthreads();
-    T.scenes = ss;
-    T.reqs = sr;
-  }
+  if(tables_in_smem) tables_to_smem(T, smem);
   const unsigned lane = threadIdx.x & 31u;
   Path p;
   p.state = ST_IDLE;
   p.flags = 0;
   p.c_seg = p.c_node = p.c_tc = 0;
-  uint32_t ri = 0, si = 0;     /* request and scene of the current path */
+  p.ri = p.si = 0;             /* request and scene of the current path */
   uint64_t wcur = 0, wend = 0; /* private chunk of the queue */
   bool drained = false;
   unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
@@ -87,7 +50,7 @@ k_persistent(PTables T, int tables_in_smem)
   for(uint32_t it = 0;; ++it) {
     const unsigned tmask = __ballot_sync(0xffffffffu, p.state == ST_TRACE);
     if(tmask && (it % period) != 0) { /* not a regrouping step: tracing lanes only */
-      if(p.state == ST_TRACE) trace_step(p, T.scenes[si]);
+      if(p.state == ST_TRACE) trace_step(p, T.scenes[p.si]);
       continue;
     }
     /* refill the private chunk of lanes that are idle with nothing left */
@@ -106,23 +69,11 @@ k_persistent(PTables T, int tables_in_smem)
         if(wcur >= T.total) { drained = true; wcur = wend = T.total; }
       }
     }
-    if(p.state == ST_IDLE && wcur < wend) {
-      const uint64_t g = wcur++;
-      const uint32_t ii = find_item(T, g);
-      const PItem item = T.items[ii];
-      ri = item.req;
-      si = item.scene;
-      const DRequest& R = T.reqs[ri];
-      const uint64_t local = g - __ldg(T.offsets + ii) + item.begin;
-      const uint32_t npix = R.width * R.height;
-      p.ireal = (uint32_t)(local / npix);
-      p.pix = (uint32_t)(local % npix);
-      p.state = ST_GEN;
-    }
+    if(p.state == ST_IDLE && wcur < wend) path_assign(p, T, wcur++);
     if(!__any_sync(0xffffffffu, p.state != ST_IDLE)) break;
     if(p.state != ST_IDLE) {
-      const DRequest& R = T.reqs[ri];
-      const DScene& S = T.scenes[si];
+      const DRequest& R = T.reqs[p.ri];
+      const DScene& S = T.scenes[p.si];
       if(p.state != ST_TRACE && p.state != ST_DONE) {
         path_event(p, S, R);
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
@@ -141,27 +92,14 @@ k_persistent(PTables T, int tables_in_smem)
     }
   }
   seg += p.c_seg; node += p.c_node; tc += p.c_tc;
-  for(int o = 16; o > 0; o >>= 1) {
-    seg += __shfl_down_sync(0xffffffffu, seg, o);
-    node += __shfl_down_sync(0xffffffffu, node, o);
-    tc += __shfl_down_sync(0xffffffffu, tc, o);
-    real += __shfl_down_sync(0xffffffffu, real, o);
-    fail += __shfl_down_sync(0xffffffffu, fail, o);
-  }
-  if(lane == 0) {
-    Counters* c = (Counters*)T.cnt;
-    atomicAdd(&c->seg, seg);
-    atomicAdd(&c->node, node);
-    atomicAdd(&c->tc, tc);
-    atomicAdd(&c->real, real);
-    atomicAdd(&c->fail, fail);
-  }
+  flush_counts(T.cnt, seg, node, tc, real, fail);
 }
 
 bool
 valid_tuning(const htrdr_gpu_tuning& t)
 {
-  return t.block_size && t.block_size <= 512 && !(t.block_size & 31) && t.queue_chunk;
+  return t.block_size && t.block_size <= 512 && !(t.block_size & 31) && t.queue_chunk
+      && (t.engine == HTRDR_GPU_ENGINE_PERSISTENT || t.engine == HTRDR_GPU_ENGINE_WAVEFRONT);
 }
 
 cudaError_t
@@ -184,6 +122,7 @@ launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
   if(blocks_per_sm) per_sm = std::min(per_sm, (int)blocks_per_sm);
   per_sm = std::max(per_sm, 1);
   k_persistent<<<(unsigned)(nsm * per_sm), block_size, smem, st>>>(T, in_smem);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -201,8 +140,22 @@ single_tables_bytes()
 }
 
 cudaError_t
-launch_persistent_single(const DScene& S, const DRequest& R, void* tables, void* cnt,
-                         const htrdr_gpu_tuning& tun, int device, cudaStream_t st)
+launch_workqueue(const PTables& T0, const htrdr_gpu_tuning& tun, WaveBufs* wave, int device,
+                 cudaStream_t st)
+{
+  PTables T = T0;
+  T.chunk = tun.queue_chunk;
+  T.regroup_period = tun.regroup_period;
+  if(tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT) {
+    if(!wave) return cudaErrorInvalidValue;
+    return launch_wavefront(T, tun, *wave, device, st);
+  }
+  return launch_persistent(T, tun.block_size, tun.blocks_per_sm, device, st);
+}
+
+cudaError_t
+launch_workqueue_single(const DScene& S, const DRequest& R, void* tables, void* cnt,
+                        const htrdr_gpu_tuning& tun, WaveBufs* wave, int device, cudaStream_t st)
 {
   SingleTables h;
   h.scene = S;
@@ -225,9 +178,7 @@ launch_persistent_single(const DScene& S, const DRequest& R, void* tables, void*
   T.total = h.offsets[1];
   T.cnt = cnt;
   T.next = (unsigned long long*)((char*)cnt + 64);
-  T.chunk = tun.queue_chunk;
-  T.regroup_period = tun.regroup_period;
-  return launch_persistent(T, tun.block_size, tun.blocks_per_sm, device, st);
+  return launch_workqueue(T, tun, wave, device, st);
 }
 
 /* Threads the persistent kernel keeps resident on the device */
@@ -252,6 +203,7 @@ struct Plan {
   DevBuf d_scenes, d_reqs, d_items, d_offsets, d_acc, d_cnt, d_out;
   size_t acc_bytes = 0;
   PTables T{};
+  WaveBufs wave; /* path slots of the wavefront engine */
 };
 
 static htrdr_gpu_res_T
@@ -326,7 +278,7 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
   return HTRDR_GPU_RES_OK;
 }
 
-/* Launch sequence of a plan: clear, persistent kernel, finalize into the
+/* Launch sequence of a plan: clear, work-queue engine, finalize into the
  * items' output buffers (device) or the plan's staging (host copies after). */
 static bool
 plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning& tun,
@@ -334,14 +286,12 @@ plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_g
 {
   bool ok = cuda_ok(cudaMemsetAsync(P.d_acc.ptr, 0, P.acc_bytes, st), "memset")
          && cuda_ok(cudaMemsetAsync(P.d_cnt.ptr, 0, 128, st), "memset");
-  PTables T = P.T;
-  T.chunk = tun.queue_chunk;
-  T.regroup_period = tun.regroup_period;
   /* inside a stream capture an event record must be an external node to time
    * the replays */
   const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   if(ok && k0) ok = cuda_ok(cudaEventRecordWithFlags(k0, st, evf), "event");
-  if(ok) ok = cuda_ok(launch_persistent(T, tun.block_size, tun.blocks_per_sm, P.device, st), "k_persistent");
+  if(ok) ok = cuda_ok(launch_workqueue(P.T, tun, &P.wave, P.device, st),
+                      tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   if(ok && k1) ok = cuda_ok(cudaEventRecordWithFlags(k1, st, evf), "event");
   for(size_t i = 0; ok && i < n; ++i) {
     char* dout = host_out ? (char*)P.d_out.ptr + P.out_off[i] : (char*)items[i].buffer;
@@ -355,12 +305,14 @@ plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_g
 }
 
 static void
-read_stats(const unsigned long long c[5], float kms, float tms, htrdr_gpu_stats* stats)
+read_stats(const unsigned long long c[5], float kms, float tms, uint64_t launches,
+           htrdr_gpu_stats* stats)
 {
   if(!stats) return;
   stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
   stats->realisations = c[3]; stats->failures = c[4];
   stats->kernel_ms = kms; stats->total_ms = tms;
+  stats->launches = launches;
 }
 
 }  // namespace hg
@@ -375,6 +327,10 @@ htrdr_gpu_default_tuning(htrdr_gpu_tuning* t)
   t->queue_chunk = 4;
   t->regroup_period = 1;
   t->blocks_per_sm = 0;
+  t->engine = HTRDR_GPU_ENGINE_PERSISTENT;
+  t->wave_slots = 0;
+  t->trace_budget = 0;
+  t->wave_tail = 0;
 }
 
 /* Best of the autotuner's grid on the LW flux and SW/CIE image workloads */
@@ -414,6 +370,7 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
   if(!items || !n) return HTRDR_GPU_RES_BAD_ARG;
   const htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
   if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
+  take_launches();
   Plan P;
   htrdr_gpu_res_T res = plan_build(P, items, n, host);
   if(res != HTRDR_GPU_RES_OK) return res;
@@ -430,7 +387,7 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
     float k = 0, t = 0;
     cudaEventElapsedTime(&k, e1, e2);
     cudaEventElapsedTime(&t, e0, e3);
-    read_stats(c, k, t, stats);
+    read_stats(c, k, t, take_launches(), stats);
   }
   cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   return ok ? HTRDR_GPU_RES_OK : HTRDR_GPU_RES_UNKNOWN_ERR;
@@ -460,23 +417,36 @@ htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best
   static const uint32_t blocks[] = {128, 256};
   static const uint32_t chunks[] = {1, 4};
   static const uint32_t periods[] = {1, 4, 16, 64};
+  static const uint32_t budgets[] = {64, 1024};
   htrdr_gpu_stats st;
   double best_t = 1e300;
   htrdr_gpu_tuning t;
   htrdr_gpu_default_tuning(&t);
   htrdr_gpu_res_T res = batched_impl(items, n, &t, &st, false); /* warm-up */
   if(res != HTRDR_GPU_RES_OK) return res;
-  for(uint32_t b : blocks)
+  auto time_it = [&](const htrdr_gpu_tuning& c) {
+    htrdr_gpu_res_T r = batched_impl(items, n, &c, &st, false);
+    if(r == HTRDR_GPU_RES_OK && st.kernel_ms < best_t) { best_t = st.kernel_ms; *best = c; }
+    return r;
+  };
+  for(uint32_t b : blocks) { /* persistent megakernel */
     for(uint32_t c : chunks)
       for(uint32_t p : periods) {
         t.block_size = b;
         t.queue_chunk = c;
         t.regroup_period = p;
-        t.blocks_per_sm = 0;
-        res = batched_impl(items, n, &t, &st, false);
-        if(res != HTRDR_GPU_RES_OK) return res;
-        if(st.kernel_ms < best_t) { best_t = st.kernel_ms; *best = t; }
+        if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
       }
+  }
+  htrdr_gpu_default_tuning(&t);
+  t.engine = HTRDR_GPU_ENGINE_WAVEFRONT;
+  for(uint32_t b : blocks) { /* wavefront: trace-stage block size x step budget */
+    for(uint32_t g : budgets) {
+      t.block_size = b;
+      t.trace_budget = g;
+      if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
+    }
+  }
   if(best_ms) *best_ms = best_t;
   return HTRDR_GPU_RES_OK;
 }
@@ -515,8 +485,14 @@ htrdr_gpu_batch_create(const htrdr_gpu_batch_item* items, size_t n, const htrdr_
                        htrdr_gpu_batch** out)
 {
   if(!items || !n || !out) return HTRDR_GPU_RES_BAD_ARG;
-  const htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
+  htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
+  if(!tuning) tun.engine = HTRDR_GPU_ENGINE_PERSISTENT; /* a mode default may name the wavefront */
   if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
+  if(tun.engine != HTRDR_GPU_ENGINE_PERSISTENT) {
+    set_error("graph batches run the persistent engine (the wavefront's iteration count is "
+              "decided on the host)");
+    return HTRDR_GPU_RES_BAD_ARG;
+  }
   auto b = new htrdr_gpu_batch();
   b->items.assign(items, items + n);
   htrdr_gpu_res_T res = plan_build(b->plan, b->items.data(), n, false);
@@ -552,6 +528,6 @@ htrdr_gpu_batch_run(htrdr_gpu_batch* b, htrdr_gpu_stats* stats)
   float k = 0, t = 0;
   cudaEventElapsedTime(&k, b->e1, b->e2);
   cudaEventElapsedTime(&t, b->e0, b->e3);
-  read_stats(c, k, t, stats);
+  read_stats(c, k, t, 1 + b->items.size(), stats); /* persistent kernel + finalizes */
   return HTRDR_GPU_RES_OK;
 }

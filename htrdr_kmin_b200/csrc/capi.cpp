@@ -10,6 +10,7 @@ namespace {
 
 struct Workspace {
   DevBuf acc, out, cnt, tables;
+  WaveBufs wave;
   size_t acc_bytes = 0, out_bytes = 0;
 };
 
@@ -57,12 +58,13 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   DRequest R;
   res = make_drequest(scn, req, &R);
   if(res != HTRDR_GPU_RES_OK) return res;
+  take_launches();
   const uint32_t npix = req->width * req->height;
   const uint32_t nch = req->mode == HG_IMAGE_CIE ? 3u : 1u;
   const size_t acc_bytes = (size_t)npix * (nch + 1) * sizeof(DAccum);
   const size_t out_bytes = layout->pitch * layout->height;
   Workspace& ws = workspace(scn);
-  const bool plain = scn->engine == HTRDR_GPU_ENGINE_PLAIN;
+  const bool plain = scn->engine_set && scn->engine == HTRDR_GPU_ENGINE_PLAIN;
   if(!ensure(ws.acc, acc_bytes) || !ensure(ws.cnt, 128)) return HTRDR_GPU_RES_MEM_ERR;
   if(!plain && !ensure(ws.tables, single_tables_bytes())) return HTRDR_GPU_RES_MEM_ERR;
   if(host && !ensure(ws.out, out_bytes)) return HTRDR_GPU_RES_MEM_ERR;
@@ -72,6 +74,7 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   htrdr_gpu_tuning tun;
   if(scn->has_tuning) tun = scn->tuning;
   else htrdr_gpu_mode_tuning(req->mode, &tun);
+  if(scn->engine_set && !plain) tun.engine = (uint32_t)scn->engine;
   cudaStream_t st = scn->stream;
   cudaEvent_t e0, e1, e2, e3;
   cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
@@ -85,8 +88,9 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   } else {
     R.acc = acc;
     R.tacc = tacc;
-    ok = ok && cuda_ok(launch_persistent_single(scn->d, R, ws.tables.ptr, ws.cnt.ptr, tun,
-                                                scn->device, st), "k_persistent");
+    ok = ok && cuda_ok(launch_workqueue_single(scn->d, R, ws.tables.ptr, ws.cnt.ptr, tun, &ws.wave,
+                                               scn->device, st),
+                       tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   }
   cudaEventRecord(e2, st);
   ok = ok && cuda_ok(launch_finalize(R, acc, tacc, dout, layout->pitch, st), "k_finalize");
@@ -103,6 +107,7 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
     stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
     stats->realisations = c[3]; stats->failures = c[4];
     stats->kernel_ms = k; stats->total_ms = t;
+    stats->launches = take_launches();
   }
   cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   return ok ? HTRDR_GPU_RES_OK : HTRDR_GPU_RES_UNKNOWN_ERR;
@@ -124,10 +129,16 @@ extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_set_engine(htrdr_gpu_scene* scn, int engine, const htrdr_gpu_tuning* tuning)
 {
   if(!scn) return HTRDR_GPU_RES_BAD_ARG;
-  if(engine != HTRDR_GPU_ENGINE_PERSISTENT && engine != HTRDR_GPU_ENGINE_PLAIN)
+  if(engine != HTRDR_GPU_ENGINE_PERSISTENT && engine != HTRDR_GPU_ENGINE_PLAIN
+  && engine != HTRDR_GPU_ENGINE_WAVEFRONT)
     return HTRDR_GPU_RES_BAD_ARG;
-  if(tuning && !valid_tuning(*tuning)) return HTRDR_GPU_RES_BAD_ARG;
+  if(tuning) {
+    htrdr_gpu_tuning t = *tuning;
+    if(engine != HTRDR_GPU_ENGINE_PLAIN) t.engine = (uint32_t)engine;
+    if(!valid_tuning(t)) return HTRDR_GPU_RES_BAD_ARG;
+  }
   scn->engine = engine;
+  scn->engine_set = 1;
   scn->has_tuning = tuning != nullptr;
   if(tuning) scn->tuning = *tuning;
   return HTRDR_GPU_RES_OK;

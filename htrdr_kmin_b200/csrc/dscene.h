@@ -21,6 +21,9 @@
 #ifndef HG_PERSIST_MAXNREG
 #define HG_PERSIST_MAXNREG 255
 #endif
+#ifndef HG_WAVE_TRACE_MAXNREG
+#define HG_WAVE_TRACE_MAXNREG 128
+#endif
 
 enum { HG_KA = 0, HG_KS = 1, HG_KEXT = 2 };
 enum { HG_XWAVE_SW = 0, HG_XWAVE_LW = 1, HG_IMAGE_CIE = 2, HG_FLUX_SW = 3, HG_FLUX_LW = 4 };

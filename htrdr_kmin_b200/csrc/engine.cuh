@@ -1,0 +1,100 @@
+/* Device pieces shared by the work-queue engines (persistent megakernel and
+ * wavefront): item lookup in the realisation index space and the FP64
+ * accumulation of a finished realisation into its request's accumulators. */
+#ifndef HTRDR_ENGINE_CUH
+#define HTRDR_ENGINE_CUH
+
+#include "internal.h"
+#include "transport.cuh"
+
+namespace {
+
+/* Item holding global realisation g: the last item whose offset is <= g */
+__device__ __forceinline__ uint32_t
+find_item(const hg::PTables& T, uint64_t g)
+{
+  uint32_t lo = 0, hi = T.nitems;
+  while(hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if(__ldg(T.offsets + mid) <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+/* Per-pixel estimator sums (src/core/htrdr_accum.h:31-68) and the
+ * realisation time, for a path in ST_DONE */
+__device__ __forceinline__ void
+accumulate_b(const Path& p, const DRequest& R)
+{
+  if(p.flags & PF_REJECTED) return;
+  const uint32_t nch = R.mode == HG_IMAGE_CIE ? 3u : 1u;
+  DAccum* a = R.acc + (size_t)p.pix * nch + p.chan;
+  if(p.flags & PF_FAILED) { atomicAdd(&a->pad, 1ull); return; }
+  atomicAdd(&a->s, p.weight);
+  atomicAdd(&a->s2, p.weight * p.weight);
+  atomicAdd(&a->n, 1ull);
+  const double us = (double)(gtimer() - p.t0) * 1e-3;
+  DAccum* t = R.tacc + p.pix;
+  atomicAdd(&t->s, us);
+  atomicAdd(&t->s2, us * us);
+  atomicAdd(&t->n, 1ull);
+}
+
+/* Start realisation `g' (global index) in path p: request, scene, pixel and
+ * realisation of the item that holds it */
+__device__ __forceinline__ void
+path_assign(Path& p, const hg::PTables& T, uint64_t g)
+{
+  const uint32_t ii = find_item(T, g);
+  const hg::PItem item = T.items[ii];
+  p.ri = item.req;
+  p.si = item.scene;
+  const DRequest& R = T.reqs[item.req];
+  const uint64_t local = g - __ldg(T.offsets + ii) + item.begin;
+  const uint32_t npix = R.width * R.height;
+  p.ireal = (uint32_t)(local / npix);
+  p.pix = (uint32_t)(local % npix);
+  p.state = ST_GEN;
+}
+
+/* Warp-wide sums of the event counters, added to the launch's totals */
+__device__ __forceinline__ void
+flush_counts(void* cnt, unsigned long long seg, unsigned long long node, unsigned long long tc,
+             unsigned long long real, unsigned long long fail)
+{
+  for(int o = 16; o > 0; o >>= 1) {
+    seg += __shfl_down_sync(0xffffffffu, seg, o);
+    node += __shfl_down_sync(0xffffffffu, node, o);
+    tc += __shfl_down_sync(0xffffffffu, tc, o);
+    real += __shfl_down_sync(0xffffffffu, real, o);
+    fail += __shfl_down_sync(0xffffffffu, fail, o);
+  }
+  if((threadIdx.x & 31u) == 0) {
+    Counters* c = (Counters*)cnt;
+    atomicAdd(&c->seg, seg);
+    atomicAdd(&c->node, node);
+    atomicAdd(&c->tc, tc);
+    atomicAdd(&c->real, real);
+    atomicAdd(&c->fail, fail);
+  }
+}
+
+/* Copy the scene and request tables of a launch into shared memory (one
+ * copy per block) and point T at them */
+__device__ __forceinline__ void
+tables_to_smem(hg::PTables& T, unsigned char* smem)
+{
+  DScene* ss = (DScene*)smem;
+  DRequest* sr = (DRequest*)(smem + ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15));
+  const uint32_t* gs = (const uint32_t*)T.scenes;
+  const uint32_t* gr = (const uint32_t*)T.reqs;
+  for(uint32_t i = threadIdx.x; i < T.nscenes * sizeof(DScene) / 4; i += blockDim.x) ((uint32_t*)ss)[i] = gs[i];
+  for(uint32_t i = threadIdx.x; i < T.nreqs * sizeof(DRequest) / 4; i += blockDim.x) ((uint32_t*)sr)[i] = gr[i];
+  __syncthreads();
+  T.scenes = ss;
+  T.reqs = sr;
+}
+
+}  // namespace
+
+#endif /* HTRDR_ENGINE_CUH */

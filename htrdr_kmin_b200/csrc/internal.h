@@ -18,6 +18,9 @@ namespace hg {
 
 void set_error(const std::string& msg);
 bool cuda_ok(cudaError_t e, const char* what);
+/* Kernel launches of the calling thread since the last take_launches() */
+void note_launches(uint64_t n);
+uint64_t take_launches();
 
 /* Device allocation owned by a scene or a request cache */
 struct DevBuf {
@@ -57,9 +60,11 @@ struct htrdr_gpu_scene {
   std::map<std::tuple<int, double, double, double>, std::unique_ptr<hg::Sampler>> samplers;
   std::mutex mtx;
   cudaStream_t stream = nullptr;
-  /* engine of draw_map on this scene (enum htrdr_gpu_engine) and the tuning
-   * of the persistent engine (has_tuning == 0: by mode) */
+  /* engine of draw_map on this scene (enum htrdr_gpu_engine; engine_set == 0:
+   * the mode's default) and the tuning of the work-queue engines
+   * (has_tuning == 0: by mode) */
   int engine = HTRDR_GPU_ENGINE_PERSISTENT;
+  int engine_set = 0;
   int has_tuning = 0;
   htrdr_gpu_tuning tuning{};
 };
@@ -147,8 +152,31 @@ uint64_t persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int de
  * `cnt' (device, 128 bytes) holds the counters and the queue head and must be
  * zeroed before the launch. */
 size_t single_tables_bytes();
-cudaError_t launch_persistent_single(const DScene& S, const DRequest& R, void* tables, void* cnt,
-                                     const htrdr_gpu_tuning& tun, int device, cudaStream_t st);
+
+/* Wavefront engine (wavefront.cu): path slots, live lists, control block and
+ * the pinned read-back of the live count, kept between runs */
+struct WaveBufs {
+  DevBuf paths, lists, ctl;
+  void* host_ctl = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  uint32_t P = 0;
+  WaveBufs() = default;
+  WaveBufs(const WaveBufs&) = delete;
+  WaveBufs& operator=(const WaveBufs&) = delete;
+  ~WaveBufs();
+};
+/* Device bytes of one path slot */
+size_t wave_slot_bytes();
+cudaError_t launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B,
+                             int device, cudaStream_t st);
+/* One launch of a work-queue engine over T: persistent kernel or wavefront
+ * (tun.engine; `wave' holds the wavefront's buffers) */
+cudaError_t launch_workqueue(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs* wave,
+                             int device, cudaStream_t st);
+/* The same for one request; the tables are staged in `tables' */
+cudaError_t launch_workqueue_single(const DScene& S, const DRequest& R, void* tables, void* cnt,
+                                    const htrdr_gpu_tuning& tun, WaveBufs* wave, int device,
+                                    cudaStream_t st);
 
 }  // namespace hg
 

@@ -258,6 +258,7 @@ launch_plain(const DScene& S, const DRequest& R, DAccum* acc, DAccum* tacc, uint
   Ra.tacc = tacc;
   k_plain<<<nblocks(total, 128), 128, 0, st>>>(S, Ra, acc, tacc, pix_begin, npix, weights,
                                                (Counters*)counters);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -270,6 +271,7 @@ launch_finalize(const DRequest& R, const DAccum* acc, const DAccum* tacc, void* 
   if(acc) Ra.acc = (DAccum*)acc;
   if(tacc) Ra.tacc = (DAccum*)tacc;
   k_finalize<<<nblocks(npix, 128), 128, 0, st>>>(Ra, acc, tacc, (char*)out, pitch);
+  note_launches(1);
   return cudaGetLastError();
 }
 

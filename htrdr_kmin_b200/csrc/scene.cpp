@@ -22,6 +22,15 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
 
+static thread_local uint64_t g_launches = 0;
+void note_launches(uint64_t n) { g_launches += n; }
+uint64_t take_launches()
+{
+  const uint64_t n = g_launches;
+  g_launches = 0;
+  return n;
+}
+
 bool
 cuda_ok(cudaError_t e, const char* what)
 {

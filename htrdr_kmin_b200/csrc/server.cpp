@@ -307,6 +307,10 @@ extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_create(const htrdr_gpu_server_config* cfg, htrdr_gpu_server** out)
 {
   if(!cfg || !out || !cfg->hbm_budget_bytes || !valid_tuning(cfg->tuning)) return HTRDR_GPU_RES_BAD_ARG;
+  if(cfg->tuning.engine != HTRDR_GPU_ENGINE_PERSISTENT) {
+    set_error("the server's rounds run the persistent engine");
+    return HTRDR_GPU_RES_BAD_ARG;
+  }
   int ndev = 0;
   if(cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
     set_error("no CUDA device available");

@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 #include <float.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "dscene.h"
@@ -393,20 +394,30 @@ struct Counters {
 };
 
 struct Path {
+  /* trace part: everything trace_step reads or writes.  It comes first so
+   * that the wavefront engine's trace stage moves only this prefix of a
+   * stored path (HG_TRACE_WORDS). */
   Rng rng;
   Trace tr;
+  uint32_t band, q, flags;
+  uint32_t si;          /* scene of the path (engines with many scenes) */
+  unsigned long long t0;
+  uint32_t c_seg, c_node, c_tc; /* local counters */
+  uint8_t state, ret, mode, chan;
+  /* event part */
   float3 org, rdir;     /* sensor ray */
   float3 pos, dir, pnext, dnext, sdir;
   double w, wdirect, inv_pdf, L_sun, weight, wlen_d;
   float ksi, tr_abs, R, refl, sun_ipdf, gdist, g, cosN, wlen;
   uint32_t bounces;
   int32_t site_cell, site_layer;
-  uint32_t pix, ireal, band, q, flags;
-  uint8_t state, ret, mode, chan;
-  unsigned long long t0;
-  /* local counters */
-  uint32_t c_seg, c_node, c_tc;
+  uint32_t pix, ireal, ri;
 };
+
+/* 32-bit words of a stored path, and of its trace part */
+#define HG_PATH_WORDS ((uint32_t)(sizeof(Path) / 4))
+#define HG_TRACE_WORDS ((uint32_t)(offsetof(Path, org) / 4))
+static_assert(sizeof(Path) % 4 == 0 && offsetof(Path, org) % 4 == 0, "word-wise path storage");
 
 __device__ __forceinline__ unsigned long long
 gtimer()

@@ -1,0 +1,465 @@
+/* Wavefront engine: the path state machine split into two stage kernels
+ * that run alternately over a pool of path slots in HBM.
+ *
+ *  - event stage (k_wave_event): for every live slot, runs path_event()
+ *    (sensor sampling, scattering and surface events, sun next-event
+ *    estimation) until the path needs a trace; a finished path is
+ *    accumulated and the slot takes the next realisation from the work
+ *    queue (path regeneration).  Slots still holding a path are compacted
+ *    into the next live list with warp-aggregated atomics; slots for which
+ *    the queue is empty drop out.
+ *  - trace stage (k_wave_trace): every resident lane takes the next live
+ *    slot, loads only the trace part of its path (a prefix of struct Path),
+ *    and steps voxels until the trace ends or a step budget is spent, then
+ *    stores the prefix back and takes another slot.  The stage holds no
+ *    event state in registers, runs none of the event code, and so keeps
+ *    more warps resident than the megakernel; lanes never wait for events.
+ *
+ * Both stages run the same state machine as the other engines on the same
+ * Philox streams, so a realisation's weight does not depend on the engine.
+ * A path is stored as contiguous 16-byte vectors per slot: the trace stage
+ * visits slots in the order lanes free up, and a lane reading its own slot's
+ * consecutive vectors uses every byte of the sectors it touches.
+ *
+ * The host drives the iterations: chunks of event+trace launches, the live
+ * count read back once per chunk (pinned memory, no device wait inside a
+ * kernel).  Every path is bounded in bounces and voxel steps, so the loop
+ * ends. */
+#include "engine.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace hg {
+
+namespace {
+
+constexpr uint32_t kPathV4 = (uint32_t)((sizeof(Path) + 15) / 16);
+constexpr uint32_t kTraceV4 = (uint32_t)((offsetof(Path, org) + 15) / 16);
+static_assert(kTraceV4 <= kPathV4, "trace part inside the path");
+
+__device__ __forceinline__ void
+load_path(Path& p, const uint4* src)
+{
+  uint4 v[kPathV4];
+#pragma unroll
+  for(uint32_t i = 0; i < kPathV4; ++i) v[i] = src[i];
+  memcpy(&p, v, sizeof(Path));
+}
+
+__device__ __forceinline__ void
+store_path(const Path& p, uint4* dst)
+{
+  uint4 v[kPathV4];
+  v[kPathV4 - 1] = make_uint4(0, 0, 0, 0);
+  memcpy(v, &p, sizeof(Path));
+#pragma unroll
+  for(uint32_t i = 0; i < kPathV4; ++i) dst[i] = v[i];
+}
+
+/* The trace part and the bytes up to the next 16-byte boundary (stored back
+ * unchanged) */
+__device__ __forceinline__ void
+load_trace(Path& p, const uint4* src)
+{
+  uint4 v[kTraceV4];
+#pragma unroll
+  for(uint32_t i = 0; i < kTraceV4; ++i) v[i] = src[i];
+  memcpy(&p, v, kTraceV4 * 16);
+}
+
+__device__ __forceinline__ void
+store_trace(const Path& p, uint4* dst)
+{
+  uint4 v[kTraceV4];
+  memcpy(v, &p, kTraceV4 * 16);
+#pragma unroll
+  for(uint32_t i = 0; i < kTraceV4; ++i) dst[i] = v[i];
+}
+
+}  // namespace
+
+/* Control block of a wavefront run (device) */
+struct WCtl {
+  uint32_t n_live[2];   /* lengths of the two live lists */
+  uint32_t fetch_event; /* next entry of the event stage's input list */
+  uint32_t fetch_trace; /* next entry of the trace stage's list */
+  uint32_t fetch_finish;/* next entry of the live list taken by the finishing megakernel */
+  uint32_t pad[3];
+};
+
+struct WTables {
+  PTables T;
+  uint4* paths;     /* [P][kPathV4] */
+  uint32_t* list0;  /* live lists, P entries each */
+  uint32_t* list1;
+  WCtl* ctl;
+  uint32_t P;
+  uint32_t budget;  /* voxel steps per trace-stage visit */
+};
+
+/* Iteration parity b: the event stage reads list b and writes list b^1; the
+ * trace stage then walks list b^1. */
+__global__ void __launch_bounds__(128)
+k_wave_event(WTables W, uint32_t b, int tables_in_smem)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  PTables T = W.T;
+  if(tables_in_smem) tables_to_smem(T, smem);
+  WCtl* ctl = W.ctl;
+  if(blockIdx.x == 0 && threadIdx.x == 0) ctl->fetch_trace = 0;
+  const uint32_t* in = b ? W.list1 : W.list0;
+  uint32_t* out = b ? W.list0 : W.list1;
+  const uint32_t n_in = ctl->n_live[b];
+  uint32_t* n_out = &ctl->n_live[b ^ 1u];
+  const unsigned lane = threadIdx.x & 31u;
+  unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
+
+  for(;;) {
+    uint32_t base = 0;
+    if(lane == 0) base = atomicAdd(&ctl->fetch_event, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if(base >= n_in) break;
+    const uint32_t idx = base + lane;
+    const bool active = idx < n_in;
+    const uint32_t s = active ? in[idx] : 0u;
+    uint4* slot = W.paths + (size_t)s * kPathV4;
+    Path p;
+    p.state = ST_IDLE;
+    if(active) {
+      load_path(p, slot);
+      p.t0 = gtimer() - p.t0; /* stored: busy time so far */
+    }
+    bool drained = !active;
+    for(;;) {
+      /* regeneration: idle lanes take the next realisations of the queue */
+      const bool need = p.state == ST_IDLE && !drained;
+      const unsigned m = __ballot_sync(0xffffffffu, need);
+      if(m) {
+        const unsigned leader = __ffs(m) - 1;
+        unsigned long long g0 = 0;
+        if(lane == leader) g0 = atomicAdd(T.next, (unsigned long long)__popc(m));
+        g0 = __shfl_sync(0xffffffffu, g0, leader);
+        if(need) {
+          const uint64_t g = g0 + __popc(m & ((1u << lane) - 1u));
+          if(g < T.total) path_assign(p, T, g);
+          else drained = true;
+        }
+      }
+      const bool busy = p.state != ST_IDLE && p.state != ST_TRACE;
+      if(!__any_sync(0xffffffffu, busy)) break;
+      if(busy) {
+        if(p.state != ST_DONE) {
+          path_event(p, T.scenes[p.si], T.reqs[p.ri]);
+          seg += p.c_seg; node += p.c_node; tc += p.c_tc;
+          p.c_seg = p.c_node = p.c_tc = 0;
+        }
+        if(p.state == ST_DONE) {
+          accumulate_b(p, T.reqs[p.ri]);
+          real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
+          fail += (p.flags & PF_FAILED) ? 1 : 0;
+          p.state = ST_IDLE;
+        }
+      }
+    }
+    const bool keep = p.state == ST_TRACE;
+    if(keep) {
+      p.t0 = gtimer() - p.t0;
+      store_path(p, slot);
+    }
+    const unsigned km = __ballot_sync(0xffffffffu, keep);
+    if(km) {
+      uint32_t pos = 0;
+      if(lane == 0) pos = atomicAdd(n_out, (uint32_t)__popc(km));
+      pos = __shfl_sync(0xffffffffu, pos, 0);
+      if(keep) out[pos + __popc(km & ((1u << lane) - 1u))] = s;
+    }
+  }
+  flush_counts(T.cnt, seg, node, tc, real, fail);
+}
+
+__global__ void __maxnreg__(HG_WAVE_TRACE_MAXNREG)
+k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  PTables T = W.T;
+  if(tables_in_smem) tables_to_smem(T, smem);
+  WCtl* ctl = W.ctl;
+  if(blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->fetch_event = 0;
+    ctl->n_live[b] = 0; /* the next event stage's output */
+  }
+  const uint32_t* list = b ? W.list0 : W.list1;
+  const uint32_t n = ctl->n_live[b ^ 1u];
+  const unsigned lane = threadIdx.x & 31u;
+  Path p;
+  p.state = ST_IDLE;
+  bool have = false, drained = false;
+  uint32_t s = 0, left = 0;
+  for(;;) {
+    const bool need = !have && !drained;
+    const unsigned m = __ballot_sync(0xffffffffu, need);
+    if(m) {
+      const unsigned leader = __ffs(m) - 1;
+      uint32_t i0 = 0;
+      if(lane == leader) i0 = atomicAdd(&ctl->fetch_trace, (uint32_t)__popc(m));
+      i0 = __shfl_sync(0xffffffffu, i0, leader);
+      if(need) {
+        const uint32_t idx = i0 + __popc(m & ((1u << lane) - 1u));
+        if(idx < n) {
+          s = list[idx];
+          load_trace(p, W.paths + (size_t)s * kPathV4);
+          p.t0 = gtimer() - p.t0;
+          have = true;
+          left = W.budget;
+        } else {
+          drained = true;
+        }
+      }
+    }
+    if(!__any_sync(0xffffffffu, have)) break;
+    if(have) {
+      trace_step(p, T.scenes[p.si]);
+      if(p.state != ST_TRACE || --left == 0) {
+        p.t0 = gtimer() - p.t0;
+        store_trace(p, W.paths + (size_t)s * kPathV4);
+        have = false;
+      }
+    }
+  }
+}
+
+/* Live list 0 = the first n0 slots, list 1 empty, counters at zero */
+__global__ void
+k_wave_init(WTables W, uint32_t n0)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i < n0) W.list0[i] = i;
+  if(i == 0) {
+    W.ctl->n_live[0] = n0;
+    W.ctl->n_live[1] = 0;
+    W.ctl->fetch_event = 0;
+    W.ctl->fetch_trace = 0;
+    W.ctl->fetch_finish = 0;
+  }
+}
+
+/* The tail of a run: once few paths are live, iterations would cost their
+ * launch and one trace's latency each while moving almost no work, so the
+ * remaining paths finish in one megakernel launch.  Lanes resume the paths of
+ * live list 0 from their slots, then take any realisations left in the work
+ * queue; events and traces run in the same thread, events regrouped every
+ * `regroup_period' voxel steps as in the persistent engine. */
+__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
+k_wave_finish(WTables W, int tables_in_smem)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  PTables T = W.T;
+  if(tables_in_smem) tables_to_smem(T, smem);
+  WCtl* ctl = W.ctl;
+  const uint32_t n = ctl->n_live[0];
+  const unsigned lane = threadIdx.x & 31u;
+  Path p;
+  p.state = ST_IDLE;
+  p.flags = 0;
+  p.c_seg = p.c_node = p.c_tc = 0;
+  p.ri = p.si = 0;
+  bool list_done = false, drained = false;
+  unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
+  const uint32_t period = T.regroup_period > 1 ? T.regroup_period : 1;
+
+  for(uint32_t it = 0;; ++it) {
+    const unsigned tmask = __ballot_sync(0xffffffffu, p.state == ST_TRACE);
+    if(tmask && (it % period) != 0) {
+      if(p.state == ST_TRACE) trace_step(p, T.scenes[p.si]);
+      continue;
+    }
+    /* idle lanes: a saved path of the live list first, then the queue */
+    const bool need_l = p.state == ST_IDLE && !list_done;
+    const unsigned ml = __ballot_sync(0xffffffffu, need_l);
+    if(ml) {
+      const unsigned leader = __ffs(ml) - 1;
+      uint32_t i0 = 0;
+      if(lane == leader) i0 = atomicAdd(&ctl->fetch_finish, (uint32_t)__popc(ml));
+      i0 = __shfl_sync(0xffffffffu, i0, leader);
+      if(need_l) {
+        const uint32_t idx = i0 + __popc(ml & ((1u << lane) - 1u));
+        if(idx < n) {
+          load_path(p, W.paths + (size_t)W.list0[idx] * kPathV4);
+          p.t0 = gtimer() - p.t0;
+        } else {
+          list_done = true;
+        }
+      }
+    }
+    const bool need_q = p.state == ST_IDLE && list_done && !drained;
+    const unsigned mq = __ballot_sync(0xffffffffu, need_q);
+    if(mq) {
+      const unsigned leader = __ffs(mq) - 1;
+      unsigned long long g0 = 0;
+      if(lane == leader) g0 = atomicAdd(T.next, (unsigned long long)__popc(mq));
+      g0 = __shfl_sync(0xffffffffu, g0, leader);
+      if(need_q) {
+        const uint64_t g = g0 + __popc(mq & ((1u << lane) - 1u));
+        if(g < T.total) path_assign(p, T, g);
+        else drained = true;
+      }
+    }
+    if(!__any_sync(0xffffffffu, p.state != ST_IDLE)) break;
+    if(p.state != ST_IDLE) {
+      const DRequest& R = T.reqs[p.ri];
+      const DScene& S = T.scenes[p.si];
+      if(p.state != ST_TRACE && p.state != ST_DONE) {
+        path_event(p, S, R);
+        seg += p.c_seg; node += p.c_node; tc += p.c_tc;
+        p.c_seg = p.c_node = p.c_tc = 0;
+      }
+      if(p.state == ST_TRACE) {
+        trace_step(p, S);
+      } else if(p.state == ST_DONE) {
+        accumulate_b(p, R);
+        real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
+        fail += (p.flags & PF_FAILED) ? 1 : 0;
+        seg += p.c_seg; node += p.c_node; tc += p.c_tc;
+        p.c_seg = p.c_node = p.c_tc = 0;
+        p.state = ST_IDLE;
+      }
+    }
+  }
+  seg += p.c_seg; node += p.c_node; tc += p.c_tc;
+  flush_counts(T.cnt, seg, node, tc, real, fail);
+}
+
+size_t
+wave_slot_bytes()
+{
+  return (size_t)kPathV4 * 16 + 2 * sizeof(uint32_t);
+}
+
+WaveBufs::~WaveBufs()
+{
+  if(host_ctl) cudaFreeHost(host_ctl);
+  if(ev[0]) cudaEventDestroy(ev[0]);
+  if(ev[1]) cudaEventDestroy(ev[1]);
+}
+
+/* Slots of a run: enough paths in flight to keep every trace lane busy
+ * several times over, no more than the realisations to render */
+static uint32_t
+wave_slots(const htrdr_gpu_tuning& tun, uint64_t total)
+{
+  uint64_t P = tun.wave_slots ? tun.wave_slots : (1u << 20);
+  if(P > total) P = total;
+  if(P < 1) P = 1;
+  return (uint32_t)P;
+}
+
+bool
+wave_reserve(WaveBufs& B, uint32_t P)
+{
+  if(!B.ctl.ptr && !B.ctl.alloc(sizeof(WCtl) * 2)) return false;
+  if(!B.host_ctl) {
+    if(!cuda_ok(cudaHostAlloc(&B.host_ctl, 2 * sizeof(WCtl), cudaHostAllocDefault), "cudaHostAlloc"))
+      return false;
+    if(!cuda_ok(cudaEventCreateWithFlags(&B.ev[0], cudaEventDisableTiming), "event")
+    || !cuda_ok(cudaEventCreateWithFlags(&B.ev[1], cudaEventDisableTiming), "event"))
+      return false;
+  }
+  if(B.P >= P && B.paths.ptr) return true;
+  if(B.paths.ptr) { cudaFree(B.paths.ptr); B.paths.ptr = nullptr; B.paths.bytes = 0; }
+  if(B.lists.ptr) { cudaFree(B.lists.ptr); B.lists.ptr = nullptr; B.lists.bytes = 0; }
+  if(!B.paths.alloc((size_t)P * kPathV4 * 16) || !B.lists.alloc((size_t)P * 2 * sizeof(uint32_t)))
+    return false;
+  B.P = P;
+  return true;
+}
+
+cudaError_t
+launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int device,
+                 cudaStream_t st)
+{
+  if(!T.total) return cudaSuccess;
+  const uint32_t P = wave_slots(tun, T.total);
+  if(!wave_reserve(B, P)) return cudaErrorMemoryAllocation;
+  const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
+  const int in_smem = tables <= 96 * 1024;
+  const size_t smem = in_smem ? tables : 0;
+  cudaError_t e;
+  if(smem > 48 * 1024) {
+    if((e = cudaFuncSetAttribute(k_wave_event, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    if((e = cudaFuncSetAttribute(k_wave_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    if((e = cudaFuncSetAttribute(k_wave_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+  }
+  int nsm = 0, ev_per_sm = 0, tr_per_sm = 0, fi_per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  const uint32_t tb = tun.block_size ? tun.block_size : 256;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ev_per_sm, k_wave_event, 128, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, k_wave_trace, (int)tb, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, k_wave_finish, (int)tb, smem);
+  if(tun.blocks_per_sm) tr_per_sm = std::min(tr_per_sm, (int)tun.blocks_per_sm);
+  const unsigned ev_grid = (unsigned)(nsm * std::max(ev_per_sm, 1));
+  const unsigned tr_grid = (unsigned)(nsm * std::max(tr_per_sm, 1));
+  const unsigned fi_grid = (unsigned)(nsm * std::max(fi_per_sm, 1));
+  /* live paths below which the rest finishes in the megakernel */
+  const uint64_t tail = tun.wave_tail ? tun.wave_tail : 4ull * fi_grid * tb;
+
+  WTables W;
+  W.T = T;
+  W.paths = (uint4*)B.paths.ptr;
+  W.list0 = (uint32_t*)B.lists.ptr;
+  W.list1 = W.list0 + P;
+  W.ctl = (WCtl*)B.ctl.ptr;
+  W.P = P;
+  W.budget = tun.trace_budget ? tun.trace_budget : 256;
+
+  /* a run too small to fill the stages is all tail: the megakernel takes the
+   * whole queue */
+  if(P < tail) {
+    k_wave_init<<<1, 32, 0, st>>>(W, 0u);
+    k_wave_finish<<<fi_grid, tb, smem, st>>>(W, in_smem);
+    note_launches(2);
+    return cudaGetLastError();
+  }
+
+  /* every slot starts idle (ST_IDLE is 0) */
+  if((e = cudaMemsetAsync(B.paths.ptr, 0, (size_t)P * kPathV4 * 16, st))) return e;
+  k_wave_init<<<(P + 255) / 256, 256, 0, st>>>(W, P);
+  note_launches(1);
+  if((e = cudaGetLastError())) return e;
+
+  /* chunks of C iterations (C even: each chunk starts at parity 0); after a
+   * chunk the live count of its last event stage (list 0) is copied back.
+   * Two chunks are in flight: the host checks chunk k-1 while chunk k runs. */
+  const uint32_t C = 8;
+  const uint64_t max_chunks = 1ull << 22;
+  WCtl* hctl = (WCtl*)B.host_ctl;
+  for(uint64_t k = 0;; ++k) {
+    if(k >= max_chunks) return cudaErrorLaunchTimeout;
+    for(uint32_t i = 0; i < C; ++i) {
+      const uint32_t b = i & 1u;
+      k_wave_event<<<ev_grid, 128, smem, st>>>(W, b, in_smem);
+      k_wave_trace<<<tr_grid, tb, smem, st>>>(W, b, in_smem);
+    }
+    note_launches(2 * C);
+    if((e = cudaGetLastError())) return e;
+    if((e = cudaMemcpyAsync(hctl + (k & 1), B.ctl.ptr, sizeof(WCtl), cudaMemcpyDeviceToHost, st)))
+      return e;
+    if((e = cudaEventRecord(B.ev[k & 1], st))) return e;
+    if(k >= 1) {
+      if((e = cudaEventSynchronize(B.ev[(k - 1) & 1]))) return e;
+      const uint32_t live = hctl[(k - 1) & 1].n_live[0];
+      if(live == 0) break; /* chunk k runs empty stages */
+      if(live < tail) {    /* after chunk k, the megakernel finishes list 0 */
+        k_wave_finish<<<fi_grid, tb, smem, st>>>(W, in_smem);
+        note_launches(1);
+        return cudaGetLastError();
+      }
+    }
+  }
+  return cudaSuccess;
+}
+
+}  // namespace hg

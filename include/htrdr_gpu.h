@@ -117,6 +117,7 @@ struct htrdr_gpu_stats {
   uint64_t failures;     /* traces stopped by the step guard */
   double kernel_ms;      /* CUDA-event time of the transport kernel(s) */
   double total_ms;       /* whole call, device side */
+  uint64_t launches;     /* kernels the call launched (transport, initialisation, finalize) */
 };
 
 struct htrdr_gpu_scene;
@@ -142,16 +143,21 @@ HTRDR_GPU_API uint32_t htrdr_gpu_scene_tree_depth(const struct htrdr_gpu_scene* 
  * Fills `buffer' (host memory, `layout') with atmosphere_pixel_{xwave,flux,image}
  * structs (src/atmosphere/htrdr_atmosphere_c.h:46-76).
  *
- * Two engines compute the same per-realisation weights (only the FP64
- * summation order of a pixel differs): the persistent kernel with its work
- * queue (default) and the plain one-thread-per-realisation kernel. ---- */
+ * Three engines compute the same per-realisation weights (only the FP64
+ * summation order of a pixel differs): the persistent megakernel with its
+ * work queue, the wavefront engine (event and trace stage kernels over a
+ * pool of path slots in HBM, same work queue) and the plain
+ * one-thread-per-realisation kernel. ---- */
 enum htrdr_gpu_engine {
   HTRDR_GPU_ENGINE_PERSISTENT = 0,
-  HTRDR_GPU_ENGINE_PLAIN = 1
+  HTRDR_GPU_ENGINE_PLAIN = 1,
+  HTRDR_GPU_ENGINE_WAVEFRONT = 2
 };
 struct htrdr_gpu_tuning;
-/* Engine of the scene's htrdr_gpu_draw_map(_device) calls; `tuning' (NULL: a
- * default by mode) applies to the persistent engine. */
+/* Engine of the scene's htrdr_gpu_draw_map(_device) calls.  `tuning' (NULL:
+ * the default of the request's mode) applies to the work-queue engines;
+ * `engine' overrides its engine field.  The default is the mode's tuning,
+ * engine included. */
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_set_engine(struct htrdr_gpu_scene* scene, int engine,
                            const struct htrdr_gpu_tuning* tuning);
@@ -223,11 +229,17 @@ struct htrdr_gpu_batch_item {
   void* buffer; /* host */
 };
 struct htrdr_gpu_tuning {
-  uint32_t block_size;    /* threads per block of the persistent kernel */
-  uint32_t queue_chunk;   /* realisations taken from the work queue at once */
+  uint32_t block_size;    /* threads per block of the persistent kernel (wavefront: of its
+                           * trace stage) */
+  uint32_t queue_chunk;   /* realisations taken from the work queue at once (persistent) */
   uint32_t regroup_period;/* voxel steps between two regroupings of a warp's lanes (events and
-                           * new realisations run together; 0 or 1: every step) */
+                           * new realisations run together; 0 or 1: every step) (persistent) */
   uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
+  uint32_t engine;        /* HTRDR_GPU_ENGINE_PERSISTENT or HTRDR_GPU_ENGINE_WAVEFRONT */
+  uint32_t wave_slots;    /* wavefront: paths in flight (0: 2^20, at most the realisations) */
+  uint32_t trace_budget;  /* wavefront: voxel steps of a trace per trace-stage visit (0: 256) */
+  uint32_t wave_tail;     /* wavefront: live paths below which the remaining ones finish in one
+                           * megakernel launch (0: four waves of its resident threads) */
 };
 /* Renders every item (each one htrdr_draw_map call of the reference) in one
  * persistent kernel; item buffers are host memory.  tuning == NULL: the
@@ -253,7 +265,9 @@ htrdr_gpu_autotune(struct htrdr_gpu_batch_item* items, size_t n, struct htrdr_gp
                    double* best_ms);
 
 /* Reusable batch (item buffers are device memory): the launch sequence is
- * captured once in a CUDA graph; every run replays it. */
+ * captured once in a CUDA graph; every run replays it.  The tuning's engine
+ * must be the persistent one (the wavefront's iteration count is decided on
+ * the host while it runs): BAD_ARG otherwise. */
 struct htrdr_gpu_batch;
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_batch_create(const struct htrdr_gpu_batch_item* items, size_t n,
@@ -275,7 +289,7 @@ struct htrdr_gpu_server_config {
   size_t hbm_budget_bytes;       /* admission budget for per-request device memory */
   double round_target_ms;        /* rounds hold ~ this much work at the observed throughput */
   uint64_t round_realisations;   /* smallest round (0: two waves of the kernel's resident threads) */
-  struct htrdr_gpu_tuning tuning;
+  struct htrdr_gpu_tuning tuning;  /* engine: the persistent one (rounds overlap on streams) */
 };
 struct htrdr_gpu_server_stats {
   uint64_t submitted, completed, failed, rounds, realisations;

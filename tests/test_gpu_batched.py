@@ -52,6 +52,53 @@ def test_batched_equals_plain(gpu_lib):
         _cmp(b, p, req.mode)
 
 
+@pytest.mark.parametrize("slots,budget,bs,tail", [
+    (0, 0, 256, 0),         # defaults: this small mix is all tail (finishing megakernel only)
+    (37, 3, 128, 1),        # stages to the end, few slots: heavy regeneration
+    (1000, 1, 64, 1),       # one voxel per trace-stage visit
+    (5000, 64, 256, 2000),  # stages, then the megakernel takes the live paths mid-run
+])
+def test_wavefront_equals_plain(gpu_lib, slots, budget, bs, tail):
+    """The wavefront engine (event and trace stages over path slots, the tail
+    finished by a megakernel that resumes the saved paths) gives the plain
+    kernel's estimates."""
+    items = _mix(gpu_lib)
+    t = gpu_lib.default_tuning()
+    t.engine, t.wave_slots, t.trace_budget, t.block_size = gpu_lib.ENGINE_WAVEFRONT, slots, budget, bs
+    t.wave_tail = tail
+    bufs, st = gpu_lib.draw_maps_batched(items, t)
+    assert st["failures"] == 0
+    ref, sref = gpu_lib.draw_maps_batched(items, gpu_lib.default_tuning())
+    assert st["realisations"] == sref["realisations"]
+    assert st["segments"] == sref["segments"] and st["collisions"] == sref["collisions"]
+    for (gs, req), b, r in zip(items, bufs, ref):
+        gs.set_engine(gpu_lib.ENGINE_PLAIN)
+        p, _ = gs.draw_map(req)
+        gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
+        _cmp(b, p, req.mode)
+        _cmp(b, r, req.mode)
+
+
+def test_wavefront_refused_where_the_host_cannot_drive_it(gpu_lib):
+    import ctypes as C
+    items = _mix(gpu_lib)[:1]
+    arr = (gpu_lib.BatchItem * 1)()
+    gs, req = items[0]
+    import torch
+    dev = torch.empty(req.width * req.height * gpu_lib.pixel_dtype(req.mode).itemsize,
+                      dtype=torch.uint8, device="cuda:0")
+    arr[0].scene, arr[0].req, arr[0].layout = gs.handle.value, gpu_lib.to_request(req), gpu_lib.layout_for(req)
+    arr[0].buffer = dev.data_ptr()
+    t = gpu_lib.default_tuning()
+    t.engine = gpu_lib.ENGINE_WAVEFRONT
+    h = C.c_void_p()
+    L = gpu_lib.lib()
+    assert L.htrdr_gpu_batch_create(arr, 1, C.byref(t), C.byref(h)) == gpu_lib.RES_BAD_ARG
+    assert b"persistent" in L.htrdr_gpu_last_error()
+    with pytest.raises(gpu_lib.HtrdrError):
+        gpu_lib.Server(device=0, hbm_budget_bytes=1 << 30, tuning=t)
+
+
 def test_draw_map_engines_agree(gpu_lib):
     """htrdr_gpu_draw_map on the persistent engine (default, by-mode or given
     tuning) equals the plain engine, on host and device outputs."""
@@ -68,6 +115,14 @@ def test_draw_map_engines_agree(gpu_lib):
         gs.set_engine(gpu_lib.ENGINE_PERSISTENT, t)
         tuned, _ = gs.draw_map(req)
         _cmp(tuned, plain, req.mode)
+        gs.set_engine(gpu_lib.ENGINE_WAVEFRONT)
+        wave, sw = gs.draw_map(req)
+        _cmp(wave, plain, req.mode)
+        assert sw["segments"] == sp["segments"]
+        t.trace_budget, t.wave_slots, t.wave_tail = 5, 333, 100
+        gs.set_engine(gpu_lib.ENGINE_WAVEFRONT, t)
+        wave2, _ = gs.draw_map(req)
+        _cmp(wave2, plain, req.mode)
         dev = torch.empty(pers.nbytes, dtype=torch.uint8, device="cuda:0")
         gs.draw_map(req, device_out=dev.data_ptr())
         torch.cuda.synchronize()

@@ -71,3 +71,12 @@ def test_engine_selection_and_mode_tuning_host_checks():
     assert (lw.block_size, lw.regroup_period) != (sw.block_size, sw.regroup_period)
     assert (sw.block_size, sw.queue_chunk, sw.regroup_period) == \
         (cie.block_size, cie.queue_chunk, cie.regroup_period)
+
+
+def test_tuning_struct_and_engine_fields():
+    # struct htrdr_gpu_tuning: eight uint32 fields, the engine among them
+    assert C.sizeof(api.Tuning) == 32
+    t = api.default_tuning()
+    assert t.engine == api.ENGINE_PERSISTENT and t.wave_slots == 0 and t.trace_budget == 0
+    for mode in (S.MODE_XWAVE_SW, S.MODE_XWAVE_LW, S.MODE_IMAGE_CIE, S.MODE_FLUX_SW, S.MODE_FLUX_LW):
+        assert api.mode_tuning(mode).engine in (api.ENGINE_PERSISTENT, api.ENGINE_WAVEFRONT)
