@@ -333,7 +333,10 @@ htrdr_gpu_default_tuning(htrdr_gpu_tuning* t)
   t->wave_tail = 0;
 }
 
-/* Best of the autotuner's grid on the LW flux and SW/CIE image workloads */
+/* Best tunings measured on a B200 for the LW flux map (persistent megakernel:
+ * short paths) and the SW and CIE images (wavefront: long multiple-scattering
+ * walks; the tail threshold is where iterations stop paying for their launch
+ * and one trace's latency) */
 extern "C" HTRDR_GPU_API void
 htrdr_gpu_mode_tuning(int mode, htrdr_gpu_tuning* t)
 {
@@ -343,10 +346,20 @@ htrdr_gpu_mode_tuning(int mode, htrdr_gpu_tuning* t)
     t->block_size = 128;
     t->queue_chunk = 1;
     t->regroup_period = 1;
-  } else {
+  } else if(mode == HG_IMAGE_CIE) {
+    t->engine = HTRDR_GPU_ENGINE_WAVEFRONT;
     t->block_size = 256;
     t->queue_chunk = 1;
     t->regroup_period = 16;
+    t->trace_budget = 256;
+    t->wave_tail = 100000;
+  } else {
+    t->engine = HTRDR_GPU_ENGINE_WAVEFRONT;
+    t->block_size = 256;
+    t->queue_chunk = 1;
+    t->regroup_period = 64;
+    t->trace_budget = 256;
+    t->wave_tail = 25000;
   }
 }
 
@@ -407,9 +420,11 @@ htrdr_gpu_draw_maps_batched_device(htrdr_gpu_batch_item* items, size_t n,
   return batched_impl(items, n, tuning, stats, false);
 }
 
-/* Autotuner of the batched engine: times every candidate (block size x queue
- * chunk x regroup period) on the given items (device buffers) with CUDA
- * events and returns the fastest.  Results do not depend on the tuning. */
+/* Autotuner: times every candidate -- persistent megakernel (block size x
+ * queue chunk x regroup period) and wavefront (tail threshold x regroup
+ * period of its finishing megakernel) -- on the given items (device buffers)
+ * with CUDA events and returns the fastest.  Results do not depend on the
+ * tuning. */
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best, double* best_ms)
 {
@@ -417,7 +432,8 @@ htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best
   static const uint32_t blocks[] = {128, 256};
   static const uint32_t chunks[] = {1, 4};
   static const uint32_t periods[] = {1, 4, 16, 64};
-  static const uint32_t budgets[] = {64, 1024};
+  static const uint32_t tails[] = {25000, 100000};
+  static const uint32_t wperiods[] = {16, 64};
   htrdr_gpu_stats st;
   double best_t = 1e300;
   htrdr_gpu_tuning t;
@@ -440,10 +456,13 @@ htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best
   }
   htrdr_gpu_default_tuning(&t);
   t.engine = HTRDR_GPU_ENGINE_WAVEFRONT;
-  for(uint32_t b : blocks) { /* wavefront: trace-stage block size x step budget */
-    for(uint32_t g : budgets) {
-      t.block_size = b;
-      t.trace_budget = g;
+  t.block_size = 256;
+  t.queue_chunk = 1;
+  t.trace_budget = 256;
+  for(uint32_t tl : tails) { /* wavefront: tail threshold x regroup period of its tail */
+    for(uint32_t p : wperiods) {
+      t.wave_tail = tl;
+      t.regroup_period = p;
       if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
     }
   }

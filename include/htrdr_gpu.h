@@ -233,7 +233,8 @@ struct htrdr_gpu_tuning {
                            * trace stage) */
   uint32_t queue_chunk;   /* realisations taken from the work queue at once (persistent) */
   uint32_t regroup_period;/* voxel steps between two regroupings of a warp's lanes (events and
-                           * new realisations run together; 0 or 1: every step) (persistent) */
+                           * new realisations run together; 0 or 1: every step) (persistent, and
+                           * the megakernel that finishes a wavefront run) */
   uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
   uint32_t engine;        /* HTRDR_GPU_ENGINE_PERSISTENT or HTRDR_GPU_ENGINE_WAVEFRONT */
   uint32_t wave_slots;    /* wavefront: paths in flight (0: 2^20, at most the realisations) */
@@ -257,9 +258,10 @@ HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
  * regrouping at every step, long SW/CIE walks larger blocks and sparser
  * regrouping. */
 HTRDR_GPU_API void htrdr_gpu_mode_tuning(int mode, struct htrdr_gpu_tuning* tuning);
-/* Autotuner: times the candidate tunings (block size, queue chunk, regroup
- * period) of the batched engine on `items' (device buffers) and returns the
- * fastest; the rendered values do not depend on the tuning. */
+/* Autotuner: times the candidate tunings (persistent: block size, queue
+ * chunk, regroup period; wavefront: tail threshold, regroup period) on
+ * `items' (device buffers) and returns the fastest; the rendered values do
+ * not depend on the tuning. */
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_autotune(struct htrdr_gpu_batch_item* items, size_t n, struct htrdr_gpu_tuning* best,
                    double* best_ms);

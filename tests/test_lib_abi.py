@@ -69,8 +69,10 @@ def test_engine_selection_and_mode_tuning_host_checks():
     for t in (lw, sw, cie):
         assert t.block_size % 32 == 0 and 0 < t.block_size <= 512 and t.queue_chunk >= 1
     assert (lw.block_size, lw.regroup_period) != (sw.block_size, sw.regroup_period)
-    assert (sw.block_size, sw.queue_chunk, sw.regroup_period) == \
-        (cie.block_size, cie.queue_chunk, cie.regroup_period)
+    # short LW paths: the persistent megakernel; long SW/CIE walks: the wavefront
+    assert lw.engine == api.ENGINE_PERSISTENT
+    assert sw.engine == cie.engine == api.ENGINE_WAVEFRONT
+    assert sw.wave_tail > 0 and cie.wave_tail > 0
 
 
 def test_tuning_struct_and_engine_fields():
