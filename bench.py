@@ -294,10 +294,7 @@ def run_serve(args):
     for i, (gs, r) in enumerate(items):
         arr[i].scene, arr[i].req, arr[i].layout = gs.handle.value, api.to_request(r), api.layout_for(r)
         arr[i].buffer = dev[i].data_ptr()
-    tuning, batched_ms = api.autotune(arr)
-    if tuning.engine != api.ENGINE_PERSISTENT:  # the server's rounds run the persistent engine
-        tuning = api.mode_tuning(S.MODE_XWAVE_SW)
-        tuning.engine = api.ENGINE_PERSISTENT
+    tuning, batched_ms = api.autotune(arr)  # the server runs the engine that wins
     for g in gss:  # the one-at-a-time arm runs the plain engine of the drop-in
         g.set_engine(api.ENGINE_PLAIN)
     plain_one = []

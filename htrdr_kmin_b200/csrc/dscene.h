@@ -68,6 +68,7 @@ struct DRequest {
   uint32_t seed;
   struct DAccum* acc;    /* [npix][channels] FP64 accumulators of this request */
   struct DAccum* tacc;   /* [npix] per-realisation time accumulators */
+  unsigned long long* ndone; /* realisations finished (serving; may be null) */
   double pix_sz[2];
   double wlen_range[2];  /* nm */
   /* wavelength sampler */

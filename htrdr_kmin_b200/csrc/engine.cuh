@@ -26,6 +26,7 @@ find_item(const hg::PTables& T, uint64_t g)
 __device__ __forceinline__ void
 accumulate_b(const Path& p, const DRequest& R)
 {
+  if(R.ndone) atomicAdd(R.ndone, 1ull); /* every realisation, rejected ones included */
   if(p.flags & PF_REJECTED) return;
   const uint32_t nch = R.mode == HG_IMAGE_CIE ? 3u : 1u;
   DAccum* a = R.acc + (size_t)p.pix * nch + p.chan;
@@ -55,6 +56,26 @@ path_assign(Path& p, const hg::PTables& T, uint64_t g)
   p.ireal = (uint32_t)(local / npix);
   p.pix = (uint32_t)(local % npix);
   p.state = ST_GEN;
+}
+
+/* Takes up to n realisations from the work queue (one atomic per warp).
+ * Returns the first index; *got is how many were taken (0: empty).  The head
+ * may pass the queued total; the wavefront's trace stage, which takes no
+ * work, clamps it back, so that work appended between chunks starts exactly
+ * at the head. */
+__device__ __forceinline__ unsigned long long
+queue_take(const hg::PTables& T, unsigned n, unsigned* got)
+{
+  const unsigned long long old = atomicAdd(T.next, (unsigned long long)n);
+  *got = old >= T.total ? 0u : (unsigned)(T.total - old < n ? T.total - old : n);
+  return old;
+}
+
+/* Head back to the queued total (one thread, while no warp takes work) */
+__device__ __forceinline__ void
+queue_clamp(const hg::PTables& T)
+{
+  if(*T.next > T.total) *T.next = T.total;
 }
 
 /* Warp-wide sums of the event counters, added to the launch's totals */

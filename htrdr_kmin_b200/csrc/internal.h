@@ -153,10 +153,21 @@ uint64_t persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int de
  * zeroed before the launch. */
 size_t single_tables_bytes();
 
+/* Control block of a wavefront run (device) */
+struct WCtl {
+  uint32_t n_live[2];   /* lengths of the two live lists */
+  uint32_t fetch_event; /* next entry of the event stage's input list */
+  uint32_t fetch_trace; /* next entry of the trace stage's list */
+  uint32_t fetch_finish;/* next entry of the live list taken by the finishing megakernel */
+  uint32_t n_dead;      /* free slots on the dead list (serving) */
+  uint32_t pad[2];
+};
+
 /* Wavefront engine (wavefront.cu): path slots, live lists, control block and
- * the pinned read-back of the live count, kept between runs */
+ * the pinned read-back of the live count, kept between runs; `dead' holds
+ * the free slots of a serving pool */
 struct WaveBufs {
-  DevBuf paths, lists, ctl;
+  DevBuf paths, lists, ctl, dead;
   void* host_ctl = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   uint32_t P = 0;
@@ -169,6 +180,18 @@ struct WaveBufs {
 size_t wave_slot_bytes();
 cudaError_t launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B,
                              int device, cudaStream_t st);
+/* Serving pool of P slots driven chunk by chunk (the caller owns the queue):
+ * reset = every slot free; revive = free slots join live list 0 (after work
+ * was appended); chunk = an even number of event+trace iterations; finish =
+ * the live paths complete in one megakernel launch, then reset.  The tail
+ * threshold is the tuning's (or its default) for these launch shapes. */
+cudaError_t wave_serve_reset(WaveBufs& B, uint32_t P, cudaStream_t st);
+cudaError_t wave_serve_revive(WaveBufs& B, cudaStream_t st);
+cudaError_t wave_serve_chunk(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int device,
+                             uint32_t iterations, cudaStream_t st);
+cudaError_t wave_serve_finish(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B,
+                              int device, cudaStream_t st);
+uint64_t wave_serve_tail(const htrdr_gpu_tuning& tun, int device);
 /* One launch of a work-queue engine over T: persistent kernel or wavefront
  * (tun.engine; `wave' holds the wavefront's buffers) */
 cudaError_t launch_workqueue(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs* wave,

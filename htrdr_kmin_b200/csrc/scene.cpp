@@ -394,6 +394,7 @@ make_drequest(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, DRequest* R)
   R->seed = req->seed;
   R->acc = nullptr;
   R->tacc = nullptr;
+  R->ndone = nullptr;
   R->pix_sz[0] = 1.0 / (double)req->width;
   R->pix_sz[1] = 1.0 / (double)req->height;
   R->wlen_range[0] = req->wlen_range[0];

@@ -49,6 +49,15 @@ struct SReq {
   int state = 0;           /* 0 pending, 1 active, 2 done */
   htrdr_gpu_res_T result = HTRDR_GPU_RES_OK;
   clk::time_point t_submit, t_done;
+  /* wavefront serving: request-table slot, scene-table slot, first chunk
+   * whose read-back covers the request, stream-ordered buffers, and the
+   * event of the map's copy to the host */
+  uint32_t rslot = 0, sslot = 0;
+  uint64_t k_admit = 0;
+  void* acc_a = nullptr;
+  void* out_a = nullptr;
+  cudaEvent_t copied = nullptr;
+  bool finishing = false;
 };
 
 /* Device resources of one round in flight */
@@ -119,6 +128,33 @@ struct htrdr_gpu_server {
 
   void loop();
   bool launch_round(Slot& s, const std::vector<SReq*>& act);
+
+  /* wavefront serving (cfg.tuning.engine == HTRDR_GPU_ENGINE_WAVEFRONT) */
+  struct Readback {
+    WCtl ctl;
+    unsigned long long next;
+    unsigned long long ndone[1]; /* [kMaxReqs] */
+  };
+  static constexpr uint32_t kMaxReqs = 4096, kMaxScenes = 256;
+  static constexpr uint64_t kMaxItems = 1u << 20;
+  WaveBufs wave;
+  uint32_t wave_P = 0;
+  uint64_t wave_tail = 0;
+  DevBuf w_scenes, w_reqs, w_items, w_offsets, w_cnt, w_ndone;
+  void* w_rb[2] = {nullptr, nullptr}; /* pinned read-backs */
+  cudaEvent_t w_ev[2] = {nullptr, nullptr}, w_ta[2] = {nullptr, nullptr}, w_tb[2] = {nullptr, nullptr};
+  std::vector<htrdr_gpu_scene*> w_scene_of;   /* scene-table slots */
+  std::vector<uint32_t> w_scene_refs;          /* active requests per scene-table slot */
+  std::vector<uint32_t> w_free_rslots;
+  uint32_t w_nreqs = 0;                        /* request-table high-water mark */
+  uint64_t w_nitems = 0, w_appended = 0;       /* queue: items and realisations appended */
+  std::vector<uint64_t> w_offsets_host;        /* [w_nitems + 1] */
+  bool w_pool_live = false;                    /* slots hold paths (not all free) */
+  void loop_wave();
+  bool wave_setup();
+  bool wave_admit(SReq* r);
+  bool wave_append(const std::vector<SReq*>& act, uint64_t budget);
+  PTables wave_tables_now();
 };
 
 /* Fair share of the round budget over the requests with work left, then the
@@ -303,14 +339,354 @@ htrdr_gpu_server::loop()
   }
 }
 
+/*******************************************************************************
+ * Wavefront serving: one pool of path slots fed by a growing work queue.
+ *
+ * Admitted requests get a slot in a device request table and stay resident;
+ * the scheduling thread appends fair-share slices of every admitted
+ * request's remaining realisations to the queue (keeping about one pool of
+ * realisations queued), and runs chunks of event+trace iterations.  Paths
+ * that end take the next queued realisation in their slot, so requests that
+ * arrive while others render start in the slots those free.  Per-request
+ * counters of finished realisations, read back after every chunk, tell when
+ * a request's map is complete (finalize, copy to the host buffer).  When no
+ * work is queued and few paths are live, the megakernel finishes them and
+ * the pool returns to all-free; a slot that finds the queue empty waits on
+ * the dead list until work is appended.
+ ******************************************************************************/
+bool
+htrdr_gpu_server::wave_setup()
+{
+  wave_P = cfg.tuning.wave_slots ? cfg.tuning.wave_slots : (1u << 20);
+  wave_tail = wave_serve_tail(cfg.tuning, cfg.device);
+  const size_t rb = sizeof(Readback) + (kMaxReqs - 1) * sizeof(unsigned long long);
+  bool ok = w_scenes.alloc(kMaxScenes * sizeof(DScene)) && w_reqs.alloc(kMaxReqs * sizeof(DRequest))
+         && w_items.alloc(kMaxItems * sizeof(PItem)) && w_offsets.alloc((kMaxItems + 1) * 8)
+         && w_cnt.alloc(128) && w_ndone.alloc(kMaxReqs * 8);
+  for(int i = 0; ok && i < 2; ++i)
+    ok = cuda_ok(cudaHostAlloc(&w_rb[i], rb, cudaHostAllocDefault), "cudaHostAlloc")
+      && cuda_ok(cudaEventCreateWithFlags(&w_ev[i], cudaEventDisableTiming), "event")
+      && cuda_ok(cudaEventCreate(&w_ta[i]), "event") && cuda_ok(cudaEventCreate(&w_tb[i]), "event");
+  ok = ok && cuda_ok(cudaMemsetAsync(w_cnt.ptr, 0, 128, io), "memset")
+          && cuda_ok(cudaMemsetAsync(w_ndone.ptr, 0, kMaxReqs * 8, io), "memset")
+          && cuda_ok(cudaMemsetAsync(w_offsets.ptr, 0, 8, io), "memset")
+          && cuda_ok(wave_serve_reset(wave, wave_P, io), "wavefront pool")
+          && cuda_ok(cudaStreamSynchronize(io), "sync");
+  w_offsets_host.assign(1, 0);
+  for(uint32_t i = kMaxReqs; i-- > 0;) w_free_rslots.push_back(i);
+  return ok;
+}
+
+/* Device memory and table entries of an admitted request (scheduling thread) */
+bool
+htrdr_gpu_server::wave_admit(SReq* r)
+{
+  uint32_t ss = 0;
+  {
+    auto it = std::find(w_scene_of.begin(), w_scene_of.end(), r->scene);
+    if(it != w_scene_of.end()) {
+      ss = (uint32_t)(it - w_scene_of.begin());
+    } else { /* a table slot no active request uses, else a new one */
+      ss = (uint32_t)w_scene_of.size();
+      for(uint32_t i = 0; i < w_scene_of.size(); ++i)
+        if(!w_scene_refs[i]) { ss = i; break; }
+      if(ss == w_scene_of.size()) {
+        if(ss >= kMaxScenes) { set_error("server: too many scenes in flight"); return false; }
+        w_scene_of.push_back(nullptr);
+        w_scene_refs.push_back(0);
+      }
+      w_scene_of[ss] = r->scene;
+    }
+  }
+  const uint32_t rs = w_free_rslots.back();
+  bool ok = cuda_ok(cudaMallocAsync(&r->acc_a, r->acc_bytes, io), "cudaMallocAsync")
+         && cuda_ok(cudaMallocAsync(&r->out_a, r->out_bytes, io), "cudaMallocAsync")
+         && cuda_ok(cudaMemsetAsync(r->acc_a, 0, r->acc_bytes, io), "memset")
+         && cuda_ok(cudaEventCreateWithFlags(&r->copied, cudaEventDisableTiming), "event");
+  if(!ok) {
+    if(r->acc_a) cudaFreeAsync(r->acc_a, io);
+    if(r->out_a) cudaFreeAsync(r->out_a, io);
+    r->acc_a = r->out_a = nullptr;
+    return false;
+  }
+  const uint32_t nch = r->dreq.mode == HG_IMAGE_CIE ? 3u : 1u;
+  r->dreq.acc = (DAccum*)r->acc_a;
+  r->dreq.tacc = r->dreq.acc + (uint64_t)r->dreq.width * r->dreq.height * nch;
+  r->dreq.ndone = (unsigned long long*)w_ndone.ptr + rs;
+  /* pageable sources are staged before the calls return */
+  ok = cuda_ok(cudaMemsetAsync(r->dreq.ndone, 0, 8, io), "memset")
+    && cuda_ok(cudaMemcpyAsync((DRequest*)w_reqs.ptr + rs, &r->dreq, sizeof(DRequest),
+                               cudaMemcpyHostToDevice, io), "H2D")
+    && cuda_ok(cudaMemcpyAsync((DScene*)w_scenes.ptr + ss, &r->scene->d, sizeof(DScene),
+                               cudaMemcpyHostToDevice, io), "H2D");
+  if(!ok) return false;
+  w_free_rslots.pop_back();
+  r->rslot = rs;
+  r->sslot = ss;
+  ++w_scene_refs[ss];
+  w_nreqs = std::max(w_nreqs, rs + 1);
+  r->next = 0;
+  return true;
+}
+
+/* Fair share of `budget' realisations over the requests with work not yet
+ * queued, then the leftovers in order; appends the items to the queue */
+bool
+htrdr_gpu_server::wave_append(const std::vector<SReq*>& act, uint64_t budget)
+{
+  std::vector<SReq*> todo;
+  for(SReq* r : act) if(r->state == 1 && r->next < r->total) todo.push_back(r);
+  if(todo.empty() || w_nitems + todo.size() > kMaxItems) return true;
+  std::vector<uint64_t> counts(todo.size(), 0);
+  uint64_t left = budget;
+  const uint64_t share = std::max<uint64_t>(1, budget / todo.size());
+  for(size_t i = 0; i < todo.size(); ++i) {
+    counts[i] = std::min(todo[i]->total - todo[i]->next, std::min(share, left));
+    left -= counts[i];
+  }
+  for(size_t i = 0; i < todo.size() && left; ++i) {
+    const uint64_t c = std::min(todo[i]->total - todo[i]->next - counts[i], left);
+    counts[i] += c;
+    left -= c;
+  }
+  std::vector<PItem> items;
+  std::vector<uint64_t> offs;
+  const uint64_t begin = w_offsets_host.back();
+  uint64_t end = begin;
+  for(size_t i = 0; i < todo.size(); ++i) {
+    if(!counts[i]) continue;
+    items.push_back(PItem{todo[i]->rslot, todo[i]->sslot, todo[i]->next});
+    end += counts[i];
+    offs.push_back(end);
+    todo[i]->next += counts[i];
+  }
+  if(items.empty()) return true;
+  const bool ok =
+    cuda_ok(cudaMemcpyAsync((PItem*)w_items.ptr + w_nitems, items.data(), items.size() * sizeof(PItem),
+                            cudaMemcpyHostToDevice, io), "H2D")
+    && cuda_ok(cudaMemcpyAsync((uint64_t*)w_offsets.ptr + w_nitems + 1, offs.data(), offs.size() * 8,
+                               cudaMemcpyHostToDevice, io), "H2D");
+  w_offsets_host.insert(w_offsets_host.end(), offs.begin(), offs.end());
+  w_nitems += items.size();
+  w_appended = end;
+  realisations += end - begin;
+  return ok;
+}
+
+PTables
+htrdr_gpu_server::wave_tables_now()
+{
+  PTables T{};
+  T.scenes = (const DScene*)w_scenes.ptr;
+  T.reqs = (const DRequest*)w_reqs.ptr;
+  T.items = (const PItem*)w_items.ptr;
+  T.offsets = (const uint64_t*)w_offsets.ptr;
+  T.nscenes = (uint32_t)w_scene_of.size();
+  T.nreqs = w_nreqs;
+  T.nitems = (uint32_t)w_nitems;
+  T.total = w_appended;
+  T.cnt = w_cnt.ptr;
+  T.next = (unsigned long long*)((char*)w_cnt.ptr + 64);
+  T.chunk = cfg.tuning.queue_chunk;
+  T.regroup_period = cfg.tuning.regroup_period;
+  return T;
+}
+
+void
+htrdr_gpu_server::loop_wave()
+{
+  cudaSetDevice(cfg.device);
+  bool failed_gpu = !wave_setup();
+  const uint32_t C = 8;       /* iterations per chunk */
+  uint64_t k = 0;             /* launches (chunks and finishes), each with a read-back */
+  bool inflight[2] = {false, false};
+  uint64_t rb_k[2] = {0, 0};  /* launch index of each read-back buffer */
+  /* the queue restarts from zero between epochs: a read-back issued in an
+   * earlier epoch holds the head of a queue that no longer exists */
+  uint64_t epoch = 0, rb_epoch[2] = {0, 0};
+  uint64_t dev_next = 0;      /* queue head and live paths at the last read-back */
+  uint32_t dev_live = 0;
+
+  /* read-back of one launch: queue head, live paths, finished requests */
+  auto process = [&](int b) -> bool {
+    if(!cuda_ok(cudaEventSynchronize(w_ev[b]), "chunk")) return false;
+    inflight[b] = false;
+    float ms = 0;
+    if(cudaEventElapsedTime(&ms, w_ta[b], w_tb[b]) == cudaSuccess) busy_ms += ms;
+    const Readback* rb = (const Readback*)w_rb[b];
+    dev_next = rb_epoch[b] == epoch ? rb->next : 0; /* else: nothing known taken yet */
+    dev_live = rb->ctl.n_live[0];
+    for(SReq* r : active) {
+      /* a read-back issued before the request was admitted holds another
+       * request's count in its table slot */
+      if(r->finishing || r->state != 1 || r->k_admit > rb_k[b] || rb->ndone[r->rslot] < r->total)
+        continue;
+      /* every realisation accumulated: the map, on the same stream */
+      const bool fin = cuda_ok(launch_finalize(r->dreq, r->dreq.acc, r->dreq.tacc, r->out_a,
+                                               r->layout.pitch, io), "k_finalize")
+                    && cuda_ok(cudaMemcpyAsync(r->host, r->out_a, r->out_bytes, cudaMemcpyDeviceToHost, io),
+                               "D2H")
+                    && cuda_ok(cudaEventRecord(r->copied, io), "event");
+      if(!fin) r->result = HTRDR_GPU_RES_UNKNOWN_ERR;
+      r->finishing = true;
+    }
+    return true;
+  };
+  /* requests whose map reached the host buffer leave */
+  auto retire = [&](bool wait) {
+    std::vector<SReq*> done;
+    for(SReq* r : active) {
+      if(!r->finishing) continue;
+      const cudaError_t q = wait ? cudaEventSynchronize(r->copied) : cudaEventQuery(r->copied);
+      if(q == cudaErrorNotReady) continue;
+      if(q != cudaSuccess) r->result = HTRDR_GPU_RES_UNKNOWN_ERR;
+      done.push_back(r);
+    }
+    for(SReq* r : done) {
+      cudaFreeAsync(r->acc_a, io);
+      cudaFreeAsync(r->out_a, io);
+      r->acc_a = r->out_a = nullptr;
+      cudaEventDestroy(r->copied);
+      r->copied = nullptr;
+      w_free_rslots.push_back(r->rslot);
+      --w_scene_refs[r->sslot];
+    }
+    std::lock_guard<std::mutex> lk(m);
+    for(SReq* r : done) {
+      hbm_used -= r->acc_bytes + r->out_bytes;
+      active.erase(std::find(active.begin(), active.end(), r));
+      finish(r, r->result);
+    }
+  };
+  /* a chunk (or the finish) into read-back buffer b */
+  auto launch = [&](int b, bool finish_all) -> bool {
+    Readback* rb = (Readback*)w_rb[b];
+    const PTables T = wave_tables_now();
+    const bool ok =
+      cuda_ok(cudaEventRecord(w_ta[b], io), "event")
+      && (finish_all ? cuda_ok(wave_serve_finish(T, cfg.tuning, wave, cfg.device, io), "wavefront finish")
+                     : cuda_ok(wave_serve_chunk(T, cfg.tuning, wave, cfg.device, C, io), "wavefront chunk"))
+      && cuda_ok(cudaEventRecord(w_tb[b], io), "event")
+      && cuda_ok(cudaMemcpyAsync(&rb->ctl, wave.ctl.ptr, sizeof(WCtl), cudaMemcpyDeviceToHost, io), "D2H")
+      && cuda_ok(cudaMemcpyAsync(&rb->next, (char*)w_cnt.ptr + 64, 8, cudaMemcpyDeviceToHost, io), "D2H")
+      && (w_nreqs == 0
+          || cuda_ok(cudaMemcpyAsync(rb->ndone, w_ndone.ptr, (size_t)w_nreqs * 8, cudaMemcpyDeviceToHost,
+                                     io), "D2H"))
+      && cuda_ok(cudaEventRecord(w_ev[b], io), "event");
+    rb_k[b] = k;
+    rb_epoch[b] = epoch;
+    inflight[b] = ok;
+    ++k;
+    ++rounds;
+    return ok;
+  };
+
+  for(;;) {
+    std::unique_lock<std::mutex> lk(m);
+    /* admission by HBM budget and request-table room, in arrival order */
+    while(!pending.empty()) {
+      SReq* r = pending.front();
+      const size_t need = r->acc_bytes + r->out_bytes;
+      if(failed_gpu) { pending.pop_front(); finish(r, HTRDR_GPU_RES_BAD_OP); continue; }
+      if(need > cfg.hbm_budget_bytes) { pending.pop_front(); finish(r, HTRDR_GPU_RES_MEM_ERR); continue; }
+      if(hbm_used + need > cfg.hbm_budget_bytes || w_free_rslots.empty()) break;
+      pending.pop_front();
+      hbm_used += need;
+      hbm_peak = std::max(hbm_peak, hbm_used);
+      lk.unlock();
+      const bool ok = wave_admit(r);
+      lk.lock();
+      if(!ok) { hbm_used -= need; finish(r, HTRDR_GPU_RES_MEM_ERR); continue; }
+      r->state = 1;
+      r->k_admit = k;
+      active.push_back(r);
+    }
+    const bool waiting = !pending.empty();
+    if(failed_gpu) { /* the device failed: every request in flight fails */
+      for(SReq* r : active) finish(r, HTRDR_GPU_RES_UNKNOWN_ERR);
+      active.clear();
+      if(stop && pending.empty()) break;
+      if(pending.empty()) cv_work.wait(lk);
+      continue;
+    }
+    lk.unlock();
+
+    /* every queued realisation was taken (the head never passes the queued
+     * total): the queue restarts from zero, which keeps the item table short.
+     * Paths in flight no longer read items; the restart is ordered after the
+     * launches in flight on the stream. */
+    if(w_nitems && dev_next >= w_appended) {
+      if(!cuda_ok(cudaMemsetAsync((char*)w_cnt.ptr + 64, 0, 8, io), "memset")) { failed_gpu = true; continue; }
+      w_nitems = 0;
+      w_appended = 0;
+      dev_next = 0;
+      w_offsets_host.assign(1, 0);
+      ++epoch;
+    }
+
+    /* keep about one pool of realisations queued */
+    bool unqueued = false;
+    for(SReq* r : active) unqueued |= r->state == 1 && r->next < r->total;
+    const uint64_t queued = w_appended > dev_next ? w_appended - dev_next : 0;
+    if(unqueued && queued < wave_P) {
+      const uint64_t before = w_appended;
+      if(!wave_append(active, wave_P - queued)) { failed_gpu = true; continue; }
+      if(w_appended > before) {
+        if(!cuda_ok(wave_serve_revive(wave, io), "revive")) { failed_gpu = true; continue; }
+        w_pool_live = true;
+      }
+    }
+
+    if(w_pool_live) { /* one chunk, then the read-back of the previous launch */
+      const int b = (int)(k & 1);
+      if(inflight[b] && !process(b)) { failed_gpu = true; continue; }
+      if(!launch(b, false)) { failed_gpu = true; continue; }
+      const int pb = b ^ 1;
+      if(inflight[pb] && !process(pb)) { failed_gpu = true; continue; }
+      retire(false);
+      /* drained: nothing queued, nothing left to queue, few live paths */
+      bool more = false;
+      for(SReq* r : active) more |= r->state == 1 && r->next < r->total;
+      if(dev_next >= w_appended && !more && !waiting) {
+        if(dev_live == 0) {
+          w_pool_live = false;
+        } else if(dev_live < wave_tail) { /* the tail: finish in the megakernel */
+          const int nb = (int)(k & 1);
+          if(inflight[nb] && !process(nb)) { failed_gpu = true; continue; }
+          if(!launch(nb, true)) { failed_gpu = true; continue; }
+          bool okp = true;
+          for(int i = 0; i < 2; ++i)
+            if(inflight[i]) okp = process(i) && okp;
+          if(!okp) { failed_gpu = true; continue; }
+          w_pool_live = false;
+        }
+      }
+      continue;
+    }
+
+    /* no live path: complete what is in flight, then wait for work */
+    bool okp = true;
+    for(int i = 0; i < 2; ++i)
+      if(inflight[i]) okp = process(i) && okp;
+    if(!okp) { failed_gpu = true; continue; }
+    bool finishing = false;
+    for(SReq* r : active) finishing |= r->finishing;
+    retire(finishing);
+    if(!active.empty()) {
+      if(!finishing) std::this_thread::sleep_for(std::chrono::microseconds(200));
+      continue;
+    }
+    lk.lock();
+    if(stop && pending.empty() && active.empty()) break;
+    if(pending.empty()) cv_work.wait(lk);
+  }
+  cudaStreamSynchronize(io);
+}
+
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_create(const htrdr_gpu_server_config* cfg, htrdr_gpu_server** out)
 {
   if(!cfg || !out || !cfg->hbm_budget_bytes || !valid_tuning(cfg->tuning)) return HTRDR_GPU_RES_BAD_ARG;
-  if(cfg->tuning.engine != HTRDR_GPU_ENGINE_PERSISTENT) {
-    set_error("the server's rounds run the persistent engine");
-    return HTRDR_GPU_RES_BAD_ARG;
-  }
   int ndev = 0;
   if(cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
     set_error("no CUDA device available");
@@ -330,7 +706,10 @@ htrdr_gpu_server_create(const htrdr_gpu_server_config* cfg, htrdr_gpu_server** o
     ok = ok && cuda_ok(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking), "stream")
             && cuda_ok(cudaEventCreate(&sl.e0), "event") && cuda_ok(cudaEventCreate(&sl.e1), "event");
   if(!ok) { htrdr_gpu_server_release(s); return HTRDR_GPU_RES_BAD_OP; }
-  s->worker = std::thread([s]() { s->loop(); });
+  if(cfg->tuning.engine == HTRDR_GPU_ENGINE_WAVEFRONT)
+    s->worker = std::thread([s]() { s->loop_wave(); });
+  else
+    s->worker = std::thread([s]() { s->loop(); });
   *out = s;
   return HTRDR_GPU_RES_OK;
 }
@@ -441,6 +820,12 @@ htrdr_gpu_server_release(htrdr_gpu_server* s)
     if(sl.e0) cudaEventDestroy(sl.e0);
     if(sl.e1) cudaEventDestroy(sl.e1);
   }
-  if(s->io) cudaStreamDestroy(s->io);
+  for(int i = 0; i < 2; ++i) {
+    if(s->w_rb[i]) cudaFreeHost(s->w_rb[i]);
+    if(s->w_ev[i]) cudaEventDestroy(s->w_ev[i]);
+    if(s->w_ta[i]) cudaEventDestroy(s->w_ta[i]);
+    if(s->w_tb[i]) cudaEventDestroy(s->w_tb[i]);
+  }
+  if(s->io) { cudaStreamSynchronize(s->io); cudaStreamDestroy(s->io); }
   delete s;
 }

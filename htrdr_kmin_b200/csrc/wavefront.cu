@@ -80,19 +80,12 @@ store_trace(const Path& p, uint4* dst)
 }  // namespace
 
 /* Control block of a wavefront run (device) */
-struct WCtl {
-  uint32_t n_live[2];   /* lengths of the two live lists */
-  uint32_t fetch_event; /* next entry of the event stage's input list */
-  uint32_t fetch_trace; /* next entry of the trace stage's list */
-  uint32_t fetch_finish;/* next entry of the live list taken by the finishing megakernel */
-  uint32_t pad[3];
-};
-
 struct WTables {
   PTables T;
   uint4* paths;     /* [P][kPathV4] */
   uint32_t* list0;  /* live lists, P entries each */
   uint32_t* list1;
+  uint32_t* dead;   /* free slots (serving: revived when work arrives), or null */
   WCtl* ctl;
   uint32_t P;
   uint32_t budget;  /* voxel steps per trace-stage visit */
@@ -138,11 +131,13 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
       if(m) {
         const unsigned leader = __ffs(m) - 1;
         unsigned long long g0 = 0;
-        if(lane == leader) g0 = atomicAdd(T.next, (unsigned long long)__popc(m));
+        unsigned got = 0;
+        if(lane == leader) g0 = queue_take(T, (unsigned)__popc(m), &got);
         g0 = __shfl_sync(0xffffffffu, g0, leader);
+        got = __shfl_sync(0xffffffffu, got, leader);
         if(need) {
-          const uint64_t g = g0 + __popc(m & ((1u << lane) - 1u));
-          if(g < T.total) path_assign(p, T, g);
+          const unsigned rank = __popc(m & ((1u << lane) - 1u));
+          if(rank < got) path_assign(p, T, g0 + rank);
           else drained = true;
         }
       }
@@ -174,6 +169,16 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
       pos = __shfl_sync(0xffffffffu, pos, 0);
       if(keep) out[pos + __popc(km & ((1u << lane) - 1u))] = s;
     }
+    /* serving: a slot left without work waits, idle, on the dead list */
+    const bool died = active && !keep && W.dead;
+    if(died) store_path(p, slot); /* p.state is ST_IDLE */
+    const unsigned dm = __ballot_sync(0xffffffffu, died);
+    if(dm) {
+      uint32_t pos = 0;
+      if(lane == 0) pos = atomicAdd(&ctl->n_dead, (uint32_t)__popc(dm));
+      pos = __shfl_sync(0xffffffffu, pos, 0);
+      if(died) W.dead[pos + __popc(dm & ((1u << lane) - 1u))] = s;
+    }
   }
   flush_counts(T.cnt, seg, node, tc, real, fail);
 }
@@ -188,6 +193,7 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
   if(blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->fetch_event = 0;
     ctl->n_live[b] = 0; /* the next event stage's output */
+    queue_clamp(T);     /* no stage takes work while this one runs */
   }
   const uint32_t* list = b ? W.list0 : W.list1;
   const uint32_t n = ctl->n_live[b ^ 1u];
@@ -241,7 +247,52 @@ k_wave_init(WTables W, uint32_t n0)
     W.ctl->fetch_event = 0;
     W.ctl->fetch_trace = 0;
     W.ctl->fetch_finish = 0;
+    W.ctl->n_dead = 0;
   }
+}
+
+/* Serving pool reset: every slot free (on the dead list), no live path */
+__global__ void
+k_wave_reset(WTables W)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i < W.P) W.dead[i] = i;
+  if(i == 0) {
+    W.ctl->n_live[0] = 0;
+    W.ctl->n_live[1] = 0;
+    W.ctl->fetch_event = 0;
+    W.ctl->fetch_trace = 0;
+    W.ctl->fetch_finish = 0;
+    W.ctl->n_dead = W.P;
+  }
+}
+
+/* Serving: new work arrived, the free slots join live list 0 (idle paths
+ * that the next event stage regenerates).  Between two chunks every slot is
+ * either on list 0 or on the dead list, so the copy stays inside list 0. */
+__global__ void
+k_wave_revive(WTables W)
+{
+  const uint32_t n = W.ctl->n_dead, base = W.ctl->n_live[0];
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if(base + i < W.P) W.list0[base + i] = W.dead[i];
+}
+
+__global__ void
+k_wave_revive_commit(WTables W)
+{
+  if(threadIdx.x == 0 && blockIdx.x == 0) {
+    const uint32_t n = W.ctl->n_live[0] + W.ctl->n_dead;
+    W.ctl->n_live[0] = n < W.P ? n : W.P;
+    W.ctl->n_dead = 0;
+  }
+}
+
+/* Queue head back to the queued total after a launch that takes work */
+__global__ void
+k_wave_clamp(WTables W)
+{
+  if(threadIdx.x == 0 && blockIdx.x == 0) queue_clamp(W.T);
 }
 
 /* The tail of a run: once few paths are live, iterations would cost their
@@ -297,11 +348,13 @@ k_wave_finish(WTables W, int tables_in_smem)
     if(mq) {
       const unsigned leader = __ffs(mq) - 1;
       unsigned long long g0 = 0;
-      if(lane == leader) g0 = atomicAdd(T.next, (unsigned long long)__popc(mq));
+      unsigned got = 0;
+      if(lane == leader) g0 = queue_take(T, (unsigned)__popc(mq), &got);
       g0 = __shfl_sync(0xffffffffu, g0, leader);
+      got = __shfl_sync(0xffffffffu, got, leader);
       if(need_q) {
-        const uint64_t g = g0 + __popc(mq & ((1u << lane) - 1u));
-        if(g < T.total) path_assign(p, T, g);
+        const unsigned rank = __popc(mq & ((1u << lane) - 1u));
+        if(rank < got) path_assign(p, T, g0 + rank);
         else drained = true;
       }
     }
@@ -374,6 +427,76 @@ wave_reserve(WaveBufs& B, uint32_t P)
   return true;
 }
 
+namespace {
+
+/* Launch shapes of a run over the tables T */
+struct WaveLaunch {
+  size_t smem = 0;
+  int in_smem = 0;
+  unsigned ev_grid = 0, tr_grid = 0, fi_grid = 0;
+  uint32_t tb = 256;
+  uint64_t tail = 0;  /* live paths below which the rest finishes in the megakernel */
+};
+
+cudaError_t
+wave_params(const PTables& T, const htrdr_gpu_tuning& tun, int device, WaveLaunch& L)
+{
+  const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
+  L.in_smem = tables <= 96 * 1024;
+  L.smem = L.in_smem ? tables : 0;
+  cudaError_t e;
+  if(L.smem > 48 * 1024) {
+    if((e = cudaFuncSetAttribute(k_wave_event, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
+      return e;
+    if((e = cudaFuncSetAttribute(k_wave_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
+      return e;
+    if((e = cudaFuncSetAttribute(k_wave_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
+      return e;
+  }
+  int nsm = 0, ev_per_sm = 0, tr_per_sm = 0, fi_per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  L.tb = tun.block_size ? tun.block_size : 256;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ev_per_sm, k_wave_event, 128, L.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, k_wave_trace, (int)L.tb, L.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, k_wave_finish, (int)L.tb, L.smem);
+  if(tun.blocks_per_sm) tr_per_sm = std::min(tr_per_sm, (int)tun.blocks_per_sm);
+  L.ev_grid = (unsigned)(nsm * std::max(ev_per_sm, 1));
+  L.tr_grid = (unsigned)(nsm * std::max(tr_per_sm, 1));
+  L.fi_grid = (unsigned)(nsm * std::max(fi_per_sm, 1));
+  L.tail = tun.wave_tail ? tun.wave_tail : 4ull * L.fi_grid * L.tb;
+  return cudaSuccess;
+}
+
+WTables
+wave_tables(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, bool serving)
+{
+  WTables W;
+  W.T = T;
+  W.paths = (uint4*)B.paths.ptr;
+  W.list0 = (uint32_t*)B.lists.ptr;
+  W.list1 = W.list0 + B.P;
+  W.dead = serving ? (uint32_t*)B.dead.ptr : nullptr;
+  W.ctl = (WCtl*)B.ctl.ptr;
+  W.P = B.P;
+  W.budget = tun.trace_budget ? tun.trace_budget : 256;
+  return W;
+}
+
+/* C iterations (C even: a chunk starts and ends at parity 0, live list 0) */
+cudaError_t
+wave_iterations(const WTables& W, const WaveLaunch& L, uint32_t C, cudaStream_t st)
+{
+  for(uint32_t i = 0; i < C; ++i) {
+    const uint32_t b = i & 1u;
+    k_wave_event<<<L.ev_grid, 128, L.smem, st>>>(W, b, L.in_smem);
+    k_wave_trace<<<L.tr_grid, L.tb, L.smem, st>>>(W, b, L.in_smem);
+  }
+  note_launches(2 * C);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t
 launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int device,
                  cudaStream_t st)
@@ -381,45 +504,17 @@ launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int
   if(!T.total) return cudaSuccess;
   const uint32_t P = wave_slots(tun, T.total);
   if(!wave_reserve(B, P)) return cudaErrorMemoryAllocation;
-  const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
-  const int in_smem = tables <= 96 * 1024;
-  const size_t smem = in_smem ? tables : 0;
-  cudaError_t e;
-  if(smem > 48 * 1024) {
-    if((e = cudaFuncSetAttribute(k_wave_event, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-    if((e = cudaFuncSetAttribute(k_wave_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-    if((e = cudaFuncSetAttribute(k_wave_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-  }
-  int nsm = 0, ev_per_sm = 0, tr_per_sm = 0, fi_per_sm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  const uint32_t tb = tun.block_size ? tun.block_size : 256;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ev_per_sm, k_wave_event, 128, smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, k_wave_trace, (int)tb, smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, k_wave_finish, (int)tb, smem);
-  if(tun.blocks_per_sm) tr_per_sm = std::min(tr_per_sm, (int)tun.blocks_per_sm);
-  const unsigned ev_grid = (unsigned)(nsm * std::max(ev_per_sm, 1));
-  const unsigned tr_grid = (unsigned)(nsm * std::max(tr_per_sm, 1));
-  const unsigned fi_grid = (unsigned)(nsm * std::max(fi_per_sm, 1));
-  /* live paths below which the rest finishes in the megakernel */
-  const uint64_t tail = tun.wave_tail ? tun.wave_tail : 4ull * fi_grid * tb;
-
-  WTables W;
-  W.T = T;
-  W.paths = (uint4*)B.paths.ptr;
-  W.list0 = (uint32_t*)B.lists.ptr;
-  W.list1 = W.list0 + P;
-  W.ctl = (WCtl*)B.ctl.ptr;
-  W.P = P;
-  W.budget = tun.trace_budget ? tun.trace_budget : 256;
+  WaveLaunch L;
+  cudaError_t e = wave_params(T, tun, device, L);
+  if(e) return e;
+  WTables W = wave_tables(T, tun, B, false);
+  W.P = P; /* the buffers may hold more slots than this run uses */
 
   /* a run too small to fill the stages is all tail: the megakernel takes the
    * whole queue */
-  if(P < tail) {
+  if(P < L.tail) {
     k_wave_init<<<1, 32, 0, st>>>(W, 0u);
-    k_wave_finish<<<fi_grid, tb, smem, st>>>(W, in_smem);
+    k_wave_finish<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
     note_launches(2);
     return cudaGetLastError();
   }
@@ -430,36 +525,96 @@ launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int
   note_launches(1);
   if((e = cudaGetLastError())) return e;
 
-  /* chunks of C iterations (C even: each chunk starts at parity 0); after a
-   * chunk the live count of its last event stage (list 0) is copied back.
-   * Two chunks are in flight: the host checks chunk k-1 while chunk k runs. */
+  /* after each chunk the live count of its last event stage (list 0) is
+   * copied back.  Two chunks are in flight: the host checks chunk k-1 while
+   * chunk k runs. */
   const uint32_t C = 8;
   const uint64_t max_chunks = 1ull << 22;
   WCtl* hctl = (WCtl*)B.host_ctl;
   for(uint64_t k = 0;; ++k) {
     if(k >= max_chunks) return cudaErrorLaunchTimeout;
-    for(uint32_t i = 0; i < C; ++i) {
-      const uint32_t b = i & 1u;
-      k_wave_event<<<ev_grid, 128, smem, st>>>(W, b, in_smem);
-      k_wave_trace<<<tr_grid, tb, smem, st>>>(W, b, in_smem);
-    }
-    note_launches(2 * C);
-    if((e = cudaGetLastError())) return e;
+    if((e = wave_iterations(W, L, C, st))) return e;
     if((e = cudaMemcpyAsync(hctl + (k & 1), B.ctl.ptr, sizeof(WCtl), cudaMemcpyDeviceToHost, st)))
       return e;
     if((e = cudaEventRecord(B.ev[k & 1], st))) return e;
     if(k >= 1) {
       if((e = cudaEventSynchronize(B.ev[(k - 1) & 1]))) return e;
       const uint32_t live = hctl[(k - 1) & 1].n_live[0];
-      if(live == 0) break; /* chunk k runs empty stages */
-      if(live < tail) {    /* after chunk k, the megakernel finishes list 0 */
-        k_wave_finish<<<fi_grid, tb, smem, st>>>(W, in_smem);
+      if(live == 0) break;  /* chunk k runs empty stages */
+      if(live < L.tail) {   /* after chunk k, the megakernel finishes list 0 */
+        k_wave_finish<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
         note_launches(1);
         return cudaGetLastError();
       }
     }
   }
   return cudaSuccess;
+}
+
+/* ---- serving: a pool of P slots driven chunk by chunk ---- */
+
+cudaError_t
+wave_serve_reset(WaveBufs& B, uint32_t P, cudaStream_t st)
+{
+  if(!wave_reserve(B, P)) return cudaErrorMemoryAllocation;
+  if(B.dead.bytes < (size_t)B.P * sizeof(uint32_t)) {
+    if(B.dead.ptr) { cudaFree(B.dead.ptr); B.dead.ptr = nullptr; B.dead.bytes = 0; }
+    if(!B.dead.alloc((size_t)B.P * sizeof(uint32_t))) return cudaErrorMemoryAllocation;
+  }
+  htrdr_gpu_tuning t;
+  htrdr_gpu_default_tuning(&t);
+  const WTables W = wave_tables(PTables{}, t, B, true);
+  cudaError_t e = cudaMemsetAsync(B.paths.ptr, 0, (size_t)B.P * kPathV4 * 16, st);
+  if(e) return e;
+  k_wave_reset<<<(B.P + 255) / 256, 256, 0, st>>>(W);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t
+wave_serve_revive(WaveBufs& B, cudaStream_t st)
+{
+  htrdr_gpu_tuning t;
+  htrdr_gpu_default_tuning(&t);
+  const WTables W = wave_tables(PTables{}, t, B, true);
+  k_wave_revive<<<std::max(1u, std::min(1024u, (B.P + 255) / 256)), 256, 0, st>>>(W);
+  k_wave_revive_commit<<<1, 32, 0, st>>>(W);
+  note_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t
+wave_serve_chunk(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int device,
+                 uint32_t iterations, cudaStream_t st)
+{
+  WaveLaunch L;
+  cudaError_t e = wave_params(T, tun, device, L);
+  if(e) return e;
+  return wave_iterations(wave_tables(T, tun, B, true), L, iterations & ~1u, st);
+}
+
+cudaError_t
+wave_serve_finish(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int device,
+                  cudaStream_t st)
+{
+  WaveLaunch L;
+  cudaError_t e = wave_params(T, tun, device, L);
+  if(e) return e;
+  const WTables W = wave_tables(T, tun, B, true);
+  k_wave_finish<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+  k_wave_clamp<<<1, 32, 0, st>>>(W);
+  note_launches(2);
+  if((e = cudaGetLastError())) return e;
+  return wave_serve_reset(B, B.P, st); /* every slot is free again */
+}
+
+uint64_t
+wave_serve_tail(const htrdr_gpu_tuning& tun, int device)
+{
+  WaveLaunch L;
+  PTables T{};
+  if(wave_params(T, tun, device, L)) return 0;
+  return L.tail;
 }
 
 }  // namespace hg

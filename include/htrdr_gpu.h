@@ -282,16 +282,21 @@ HTRDR_GPU_API void htrdr_gpu_batch_release(struct htrdr_gpu_batch* batch);
  * Requests (scene, request, layout, host buffer) are submitted at any time.
  * A scheduling thread admits them while their device memory (FP64
  * accumulators + output staging) fits in the HBM budget, keeps their
- * accumulators resident, and launches rounds of the persistent kernel over a
- * share of every admitted request's remaining realisations; requests that
- * arrive while a round runs join the next one.  A request completes when all
- * its realisations are accumulated: its map is copied to its host buffer. */
+ * accumulators resident, and feeds a fair share of every admitted request's
+ * remaining realisations to the engine: rounds of the persistent kernel, or
+ * the wavefront's work queue, whose path slots take the realisations of newly
+ * admitted requests as soon as their paths end.  Requests that arrive while
+ * others render join the running work.  A request completes when all its
+ * realisations are accumulated: its map is copied to its host buffer. */
 struct htrdr_gpu_server_config {
   int device;
   size_t hbm_budget_bytes;       /* admission budget for per-request device memory */
   double round_target_ms;        /* rounds hold ~ this much work at the observed throughput */
   uint64_t round_realisations;   /* smallest round (0: two waves of the kernel's resident threads) */
-  struct htrdr_gpu_tuning tuning;  /* engine: the persistent one (rounds overlap on streams) */
+  struct htrdr_gpu_tuning tuning;  /* persistent: rounds of the megakernel on three streams;
+                                    * wavefront: one pool of path slots fed by a growing
+                                    * queue (wave_slots paths, held for the server's
+                                    * lifetime) */
 };
 struct htrdr_gpu_server_stats {
   uint64_t submitted, completed, failed, rounds, realisations;

@@ -95,8 +95,6 @@ def test_wavefront_refused_where_the_host_cannot_drive_it(gpu_lib):
     L = gpu_lib.lib()
     assert L.htrdr_gpu_batch_create(arr, 1, C.byref(t), C.byref(h)) == gpu_lib.RES_BAD_ARG
     assert b"persistent" in L.htrdr_gpu_last_error()
-    with pytest.raises(gpu_lib.HtrdrError):
-        gpu_lib.Server(device=0, hbm_budget_bytes=1 << 30, tuning=t)
 
 
 def test_draw_map_engines_agree(gpu_lib):

@@ -46,10 +46,32 @@ def mix(gpu_lib):
     return reqs
 
 
-def test_server_results_equal_alone(gpu_lib, mix):
+def _tuning(api, engine, slots=0, tail=0):
+    """Server tuning: the persistent rounds, or the wavefront slot pool (few
+    slots: regeneration, revival of free slots and queue refills all occur)"""
+    t = api.default_tuning()
+    t.engine = engine
+    if engine == api.ENGINE_WAVEFRONT:
+        t.block_size, t.regroup_period, t.wave_slots, t.wave_tail = 128, 4, slots, tail
+    return t
+
+
+# (name, slots, tail): the wavefront pool finishes its tail in the megakernel
+# (tail 0: default threshold) or runs the stages to the end (tail 1)
+ENGINES = [("persistent", 0, 0), ("wavefront", 3000, 0), ("wavefront_no_tail", 2000, 1)]
+WAIT_S = 120.0
+
+
+def _engine(api, name):
+    return api.ENGINE_PERSISTENT if name == "persistent" else api.ENGINE_WAVEFRONT
+
+
+@pytest.mark.parametrize("name,slots,tail", ENGINES)
+def test_server_results_equal_alone(gpu_lib, mix, name, slots, tail):
     api = gpu_lib
     alone = [gs.draw_map(r)[0] for gs, r in mix]
-    srv = api.Server(round_target_ms=2.0, round_realisations=4096)
+    srv = api.Server(round_target_ms=2.0, round_realisations=4096,
+                     tuning=_tuning(api, _engine(api, name), slots, tail))
     tickets = [None] * len(mix)
 
     def submitter(idx):
@@ -63,7 +85,7 @@ def test_server_results_equal_alone(gpu_lib, mix):
         t.start()
     for t in ts:
         t.join()
-    out = [srv.wait(t) for t in tickets]
+    out = [srv.wait(t, WAIT_S) for t in tickets]
     st = srv.stats()
     srv.close()
     assert st["completed"] == len(mix) and st["failed"] == 0
@@ -73,20 +95,40 @@ def test_server_results_equal_alone(gpu_lib, mix):
         _cmp(a, b, r.mode)
 
 
-def test_server_admission_by_budget(gpu_lib, mix):
+@pytest.mark.parametrize("name,slots,tail", ENGINES[:2])
+def test_server_admission_by_budget(gpu_lib, mix, name, slots, tail):
     api = gpu_lib
     sizes = []
     for gs, r in mix:
         nch = 3 if r.mode == S.MODE_IMAGE_CIE else 1
         sizes.append(r.width * r.height * (nch + 1) * 32 + r.width * r.height * r.pixel_size)
     budget = max(sizes) + 16
-    srv = api.Server(hbm_budget_bytes=budget, round_target_ms=2.0, round_realisations=2048)
+    srv = api.Server(hbm_budget_bytes=budget, round_target_ms=2.0, round_realisations=2048,
+                     tuning=_tuning(api, _engine(api, name), slots, tail))
     tickets = [srv.submit(gs, r) for gs, r in mix]
-    out = [srv.wait(t) for t in tickets]
+    out = [srv.wait(t, WAIT_S) for t in tickets]
     st = srv.stats()
     srv.close()
     assert st["hbm_peak_bytes"] <= budget
     for (gs, r), a in zip(mix, out):
+        _cmp(a, gs.draw_map(r)[0], r.mode)
+
+
+def test_wavefront_server_after_idle(gpu_lib, mix):
+    """Two bursts with an idle gap: the pool drains, the queue restarts from
+    zero, free slots are revived for the second burst, and every map equals
+    its rendering alone."""
+    api = gpu_lib
+    srv = api.Server(tuning=_tuning(api, api.ENGINE_WAVEFRONT, 1500, 0))
+    first = [srv.submit(gs, r) for gs, r in mix[:5]]
+    out1 = [srv.wait(t, WAIT_S) for t in first]
+    time.sleep(0.2)
+    second = [srv.submit(gs, r) for gs, r in mix[5:]]
+    out2 = [srv.wait(t, WAIT_S) for t in second]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(mix) and st["failed"] == 0
+    for (gs, r), a in zip(mix, out1 + out2):
         _cmp(a, gs.draw_map(r)[0], r.mode)
 
 
