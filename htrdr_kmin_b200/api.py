@@ -42,6 +42,7 @@ EXPORTED = [
     "htrdr_gpu_server_stats", "htrdr_gpu_server_release",
     "htrdr_gpu_default_tuning", "htrdr_gpu_version", "htrdr_gpu_device_count",
     "htrdr_gpu_last_error", "htrdr_gpu_scene_set_engine", "htrdr_gpu_mode_tuning",
+    "htrdr_gpu_write_image",
 ]
 
 ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT = 0, 1, 2
@@ -119,6 +120,15 @@ class ServerConfig(C.Structure):
                 ("tuning", Tuning)]
 
 
+class MapSummary(C.Structure):
+    _fields_ = [("path_time_E", C.c_double), ("path_time_SE", C.c_double),
+                ("flux_E", C.c_double), ("flux_SE", C.c_double),
+                ("path_time_n", C.c_uint64), ("flux_n", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("rounds", C.c_uint64), ("realisations", C.c_uint64), ("p50_ms", C.c_double),
@@ -193,6 +203,8 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_mode_tuning.argtypes = [i32, C.POINTER(Tuning)]
     L.htrdr_gpu_mode_tuning.restype = None
     L.htrdr_gpu_scene_set_engine.argtypes = [vp, i32, C.POINTER(Tuning)]
+    L.htrdr_gpu_write_image.argtypes = [i32, C.POINTER(BufferLayout), vp, C.c_char_p,
+                                        C.POINTER(MapSummary)]
     L.htrdr_gpu_version.restype = C.c_char_p
     L.htrdr_gpu_last_error.restype = C.c_char_p
     L.htrdr_gpu_device_count.restype = C.c_int
@@ -404,6 +416,21 @@ class GpuScene:
                                                  _ptr(r1), _ptr(cb), _ptr(wl), _ptr(pdf)),
                "sample_wavelength")
         return cb, wl, pdf
+
+
+def write_image(mode: int, buf: np.ndarray, path: str) -> dict:
+    """Write a map (the pixel buffer draw_map returns) as an htrdr-image file;
+    returns the run summaries (time per path, flux density)."""
+    lay = BufferLayout()
+    lay.width, lay.height = buf.shape[1], buf.shape[0]
+    lay.elmt_size = buf.dtype.itemsize
+    lay.pitch = buf.shape[1] * buf.dtype.itemsize
+    lay.alignment = 8
+    b = np.ascontiguousarray(buf)
+    sm = MapSummary()
+    _check(lib().htrdr_gpu_write_image(mode, C.byref(lay), b.ctypes.data, path.encode(), C.byref(sm)),
+           "htrdr_gpu_write_image")
+    return sm.as_dict()
 
 
 def default_tuning() -> Tuning:

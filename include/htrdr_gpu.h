@@ -184,6 +184,21 @@ HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_map_noalloc(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
                            const struct htrdr_gpu_buffer_layout* layout, void* device_buffer);
 
+/* ---- output: the htrdr-image file of a map and the run summaries
+ * (dump_buffer and atmosphere_draw_map, src/atmosphere/htrdr_atmosphere_draw_map.c:477-641;
+ * format doc/htrdr-image.5).  `buffer' holds the map (host memory, `layout')
+ * in the pixel structs of `mode'; `path' is a file name or "-" for stdout.
+ * summary (may be NULL): the estimates of the time per radiative path (us)
+ * and, for flux maps, of the flux density over all pixels' weights. ---- */
+struct htrdr_gpu_map_summary {
+  double path_time_E, path_time_SE;
+  double flux_E, flux_SE;
+  uint64_t path_time_n, flux_n;
+};
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_write_image(int mode, const struct htrdr_gpu_buffer_layout* layout, const void* buffer,
+                      const char* path, struct htrdr_gpu_map_summary* summary);
+
 /* ---- radiance routines, batched: atmosphere_compute_radiance_sw / _lw
  * (src/atmosphere/htrdr_atmosphere_c.h:140-163).  Ray i uses the random
  * stream keyed by (i, seed).  out[i] in W/m^2/sr/m. ---- */
