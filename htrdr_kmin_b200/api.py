@@ -42,7 +42,7 @@ EXPORTED = [
     "htrdr_gpu_server_stats", "htrdr_gpu_server_release",
     "htrdr_gpu_default_tuning", "htrdr_gpu_version", "htrdr_gpu_device_count",
     "htrdr_gpu_last_error", "htrdr_gpu_scene_set_engine", "htrdr_gpu_mode_tuning",
-    "htrdr_gpu_write_image",
+    "htrdr_gpu_write_image", "htrdr_gpu_ground_trace",
 ]
 
 ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT = 0, 1, 2
@@ -70,6 +70,13 @@ class SceneDesc(C.Structure):
         ("ground_reflectivity", C.c_double), ("ground_temperature", C.c_double),
         ("sun_azimuth", C.c_double), ("sun_elevation", C.c_double),
         ("props_mask", C.c_uint32), ("octree_on_host", C.c_int32),
+        ("ground_nverts", C.c_uint32), ("ground_verts", C.POINTER(C.c_float)),
+        ("ground_ntris", C.c_uint32), ("ground_tris", C.POINTER(C.c_uint32)),
+        ("ground_tri_iface", C.POINTER(C.c_uint32)), ("ground_nifaces", C.c_uint32),
+        ("ground_ifaces", C.POINTER(C.c_uint32)), ("ground_nmtls", C.c_uint32),
+        ("ground_mtl_temperature", C.POINTER(C.c_double)),
+        ("ground_mtl_nbrdf", C.POINTER(C.c_uint32)), ("ground_mtl_brdf", C.POINTER(C.c_double)),
+        ("repeat_ground", C.c_int32), ("ground_sky_mtl", C.c_uint32),
     ]
 
 
@@ -205,6 +212,7 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_scene_set_engine.argtypes = [vp, i32, C.POINTER(Tuning)]
     L.htrdr_gpu_write_image.argtypes = [i32, C.POINTER(BufferLayout), vp, C.c_char_p,
                                         C.POINTER(MapSummary)]
+    L.htrdr_gpu_ground_trace.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp]
     L.htrdr_gpu_version.restype = C.c_char_p
     L.htrdr_gpu_last_error.restype = C.c_char_p
     L.htrdr_gpu_device_count.restype = C.c_int
@@ -299,6 +307,8 @@ class GpuScene:
         d.sun_elevation = scene.sun_elevation
         d.props_mask = props_mask
         d.octree_on_host = int(octree_on_host)
+        if scene.ground_mesh is not None:
+            scene.ground_mesh.fill_desc(d, keep)
         h = C.c_void_p()
         _check(lib().htrdr_gpu_scene_create(device, C.byref(d), C.byref(h)), "htrdr_gpu_scene_create")
         self.handle = h
@@ -352,6 +362,22 @@ class GpuScene:
         _check(lib().htrdr_gpu_draw_map(self.handle, C.byref(r), C.byref(lay), _ptr(buf), C.byref(st)),
                "htrdr_gpu_draw_map")
         return buf, st.as_dict()
+
+    def ground_trace(self, rays: np.ndarray, tmax: np.ndarray, from_prim: np.ndarray,
+                     from_edge: np.ndarray):
+        """Ground queries on the mesh: rays [n, 6] float32 (origin, direction),
+        range [0, tmax), the primitive each ray leaves (NO_ID: none) and
+        whether that hit lay on an edge.  Returns (primitive, distance)."""
+        n = rays.shape[0]
+        r = np.ascontiguousarray(rays, dtype=np.float32)
+        t = np.ascontiguousarray(tmax, dtype=np.float32)
+        fp = np.ascontiguousarray(from_prim, dtype=np.uint32)
+        fe = np.ascontiguousarray(from_edge, dtype=np.uint8)
+        prim = np.zeros(n, np.uint32)
+        dist = np.zeros(n, np.float32)
+        _check(lib().htrdr_gpu_ground_trace(self.handle, n, _ptr(r), _ptr(t), _ptr(fp), _ptr(fe),
+                                            _ptr(prim), _ptr(dist)), "htrdr_gpu_ground_trace")
+        return prim, dist
 
     def realisation_weights(self, req: S.Request, pix_begin: int, pix_end: int) -> np.ndarray:
         out = np.zeros((pix_end - pix_begin, req.realisations_per_pixel), np.float64)

@@ -272,6 +272,28 @@ htrdr_gpu_locate_leaf(htrdr_gpu_scene* scn, uint32_t iband, uint32_t iquad, int 
 }
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_ground_trace(htrdr_gpu_scene* scn, size_t n, const float* rays, const float* tmax,
+                       const uint32_t* from_prim, const uint8_t* from_edge, uint32_t* prim,
+                       float* dist)
+{
+  if(!scn || !scn->d.g_ntris) return HTRDR_GPU_RES_BAD_ARG;
+  if(n && (!rays || !tmax || !from_prim || !from_edge || !prim || !dist)) return HTRDR_GPU_RES_BAD_ARG;
+  if(!n) return HTRDR_GPU_RES_OK;
+  if(!cuda_ok(cudaSetDevice(scn->device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
+  DevArr<float> dr, dt, dd;
+  DevArr<uint32_t> df, dp;
+  DevArr<uint8_t> de;
+  if(!dr.from(rays, 6 * n) || !dt.from(tmax, n) || !df.from(from_prim, n) || !de.from(from_edge, n)
+  || !dp.make(n) || !dd.make(n))
+    return HTRDR_GPU_RES_MEM_ERR;
+  if(!cuda_ok(launch_ground_trace(scn->d, n, dr.p(), dt.p(), df.p(), de.p(), dp.p(), dd.p(),
+                                  scn->stream), "k_ground_trace")
+  || !cuda_ok(cudaStreamSynchronize(scn->stream), "sync") || !dp.to(prim, n) || !dd.to(dist, n))
+    return HTRDR_GPU_RES_UNKNOWN_ERR;
+  return HTRDR_GPU_RES_OK;
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_sample_wavelength(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, int channel,
                             size_t n, const double* r0, const double* r1, uint32_t* cdf_band,
                             double* wlen, double* pdf)

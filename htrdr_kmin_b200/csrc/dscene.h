@@ -12,6 +12,7 @@
 #define HG_MAX_STEPS (1u << 20)   /* voxel steps per trace before giving up */
 #define HG_MAX_BOUNCES (1u << 16) /* scattering events per realisation before giving up */
 #define HG_MAX_NULL (1u << 22)    /* tentative collisions per voxel before giving up */
+#define HG_BVH_DEPTH_MAX 48       /* ground BVH depth bound (the traversal stack size) */
 
 /* Register budget of the transport kernels (per thread): trades occupancy
  * against spills of the per-path state. */
@@ -56,6 +57,20 @@ struct DScene {
   /* ground */
   int32_t has_ground, ground_brdf;
   float ground_refl, ground_T;
+  /* ground mesh (g_ntris > 0 replaces the plane ground) */
+  uint32_t g_ntris, g_nmtls;
+  int32_t g_repeat;
+  uint32_t g_sky_mtl;         /* material of the atmosphere (~0u: none) */
+  const float4* g_tri;        /* [ntris][3] v0, v1, v2 in BVH order (w unused) */
+  const uint32_t* g_tri_id;   /* [ntris] BVH order -> primitive id of the caller */
+  const uint32_t* g_iface_of; /* [ntris] interface of each primitive id */
+  const uint4* g_iface;       /* [nifaces] {front, thin, back, 0} material (~0u: none) */
+  const float4* g_bvh;        /* [nodes][2] {lo, first/left}, {hi, count (0: inner)} */
+  const uint2* g_mtl;         /* [nmtls] {first brdf, nbrdf} */
+  const float* g_mtl_T;       /* [nmtls] K */
+  const double* g_brdf_wl;    /* [nbrdf] nm */
+  const float2* g_brdf;       /* [nbrdf] {type, reflectivity} */
+  double g_lower[3], g_upper[3]; /* mesh bounding box (the repeated cell) */
   /* sun */
   float sun_dir[3], sun_b1[3], sun_b2[3];
   double sun_dir_d[3];

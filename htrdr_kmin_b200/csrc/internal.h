@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -91,6 +92,11 @@ void build_octree(const DScene& hs, const float* lwc, const float* sig3, const f
                   uint32_t depth, uint32_t level_force, double tau, double cmax,
                   std::vector<uint32_t>& nodes);
 
+/* Ground mesh: validation, BVH and device tables into S (ground.cpp);
+ * `upload' copies a host array to a device buffer owned by the scene */
+htrdr_gpu_res_T setup_ground_mesh(const htrdr_gpu_scene_desc* desc, DScene& S,
+                                  const std::function<void*(const void*, size_t)>& upload);
+
 /* Octree build on the GPU (octree_gpu.cu), node arrays identical to build_octree */
 bool build_octrees_gpu(const DScene& S, const float* d_lwc, const int2* d_cl, const float* d_gka,
                        const float* d_gks, const std::vector<float>& sig3,
@@ -117,6 +123,9 @@ cudaError_t launch_find_band(const DScene& S, size_t n, const double* wlen, uint
                              cudaStream_t st);
 cudaError_t launch_sample_quad(const DScene& S, size_t n, const double* r, const uint32_t* band,
                                uint32_t* out, cudaStream_t st);
+cudaError_t launch_ground_trace(const DScene& S, size_t n, const float* rays, const float* tmax,
+                                const uint32_t* from_prim, const uint8_t* from_edge, uint32_t* prim,
+                                float* dist, cudaStream_t st);
 cudaError_t launch_locate_leaf(const DScene& S, uint32_t q, int prop, size_t n,
                                const uint32_t* cells, uint32_t* node, uint32_t* level,
                                cudaStream_t st);

@@ -208,6 +208,19 @@ k_sample_quad(DScene S, size_t n, const double* r, const uint32_t* band, uint32_
 }
 
 __global__ void
+k_ground_trace(DScene S, size_t n, const float* rays, const float* tmax, const uint32_t* from_prim,
+               const uint8_t* from_edge, uint32_t* prim, float* dist)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  const float3 o = make_float3(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+  const float3 d = make_float3(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+  const GHit h = g_trace(S, o, d, 0.f, tmax[i], from_prim[i], from_edge[i] != 0);
+  prim[i] = h.prim;
+  dist[i] = h.prim == HG_NO_PRIM ? -1.f : h.dist;
+}
+
+__global__ void
 k_locate_leaf(DScene S, uint32_t q, int prop, size_t n, const uint32_t* cells, uint32_t* node,
               uint32_t* level)
 {
@@ -299,6 +312,16 @@ launch_sample_quad(const DScene& S, size_t n, const double* r, const uint32_t* b
 {
   if(!n) return cudaSuccess;
   k_sample_quad<<<nblocks(n, 256), 256, 0, st>>>(S, n, r, band, out);
+  return cudaGetLastError();
+}
+
+cudaError_t
+launch_ground_trace(const DScene& S, size_t n, const float* rays, const float* tmax,
+                    const uint32_t* from_prim, const uint8_t* from_edge, uint32_t* prim, float* dist,
+                    cudaStream_t st)
+{
+  if(!n) return cudaSuccess;
+  k_ground_trace<<<nblocks(n, 128), 128, 0, st>>>(S, n, rays, tmax, from_prim, from_edge, prim, dist);
   return cudaGetLastError();
 }
 

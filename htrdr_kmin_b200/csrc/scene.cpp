@@ -673,6 +673,10 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
   S.ground_brdf = desc->ground_brdf;
   S.ground_refl = (float)desc->ground_reflectivity;
   S.ground_T = (float)desc->ground_temperature;
+  {
+    const htrdr_gpu_res_T res = setup_ground_mesh(desc, S, upload);
+    if(res != HTRDR_GPU_RES_OK) return res;
+  }
   { /* sun (src/atmosphere/htrdr_atmosphere_sun.c:66-101) */
     const double pi = 3.14159265358979323846;
     const double az = desc->sun_azimuth * pi / 180.0, el = desc->sun_elevation * pi / 180.0;

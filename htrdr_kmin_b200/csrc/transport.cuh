@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include "dscene.h"
+#include "ground.cuh"
 
 #define HG_PI_D 3.14159265358979323846
 #define HG_PI_F 3.14159265358979323846f
@@ -346,6 +347,68 @@ ground_trace(const DScene& S, float3 o, float3 d, float r0, float r1, bool prev_
   return (t <= r0 || t >= r1) ? -1.f : t;
 }
 
+/* Ground query of the walk, on the mesh when the scene has one, else on the
+ * plane: distance in [0, r1) (< 0: none), the hit primitive, whether the hit
+ * lies on an edge and the geometric normal.  `prev' says the ray leaves the
+ * ground at (prev_prim, prev_edge). */
+__device__ __forceinline__ float
+ground_query(const DScene& S, float3 o, float3 d, float r1, bool prev, uint32_t prev_prim,
+             bool prev_edge, uint32_t* prim, bool* edge, float3* ng)
+{
+  if(!S.g_ntris) {
+    *prim = 0;
+    *edge = false;
+    *ng = make_float3(0.f, 0.f, 1.f);
+    return ground_trace(S, o, d, 0.f, r1, prev);
+  }
+  const GHit h = g_trace(S, o, d, 0.f, r1, prev ? prev_prim : HG_NO_PRIM, prev && prev_edge);
+  *prim = h.prim;
+  *edge = h.prim != HG_NO_PRIM && g_on_edge(h.u, h.v);
+  *ng = h.ng;
+  return h.prim == HG_NO_PRIM ? -1.f : h.dist;
+}
+
+/* Ground properties at a surface event: the normal (unoriented), the BRDF
+ * type and reflectivity and the temperature.  On the mesh, the material of
+ * the hit side's interface and the BRDF tabulated at the wavelength, chosen
+ * with one transport canonical as htrdr_mtl_create_bsdf does
+ * (src/core/htrdr_materials.c:414-463); on the plane, its constants and no
+ * draw.  A side without a BRDF reflects nothing. */
+struct SurfProps {
+  float3 N;
+  float refl, T;
+  int specular;
+};
+
+__device__ __forceinline__ SurfProps
+surface_props(const DScene& S, Rng& rng, float3 dir, uint32_t prim, float3 ng, double wlen_nm)
+{
+  SurfProps s;
+  if(!S.g_ntris) {
+    s.N = make_float3(0.f, 0.f, 1.f);
+    s.refl = S.ground_refl;
+    s.specular = S.ground_brdf == 1;
+    s.T = S.ground_T;
+    return s;
+  }
+  const float n = rsqrtf(ng.x * ng.x + ng.y * ng.y + ng.z * ng.z);
+  s.N = make_float3(ng.x * n, ng.y * n, ng.z * n);
+  const uint32_t m = g_hit_mtl(S, prim, ng, dir);
+  const double r = (double)rng.uf();
+  const uint32_t b = m == HG_NO_PRIM ? HG_NO_PRIM : g_fetch_brdf(S, m, wlen_nm, r);
+  if(b == HG_NO_PRIM) {
+    s.refl = 0.f;
+    s.specular = 0;
+    s.T = m == HG_NO_PRIM ? 0.f : __ldg(S.g_mtl_T + m);
+    return s;
+  }
+  const float2 br = __ldg(S.g_brdf + b);
+  s.specular = br.x != 0.f;
+  s.refl = br.y;
+  s.T = __ldg(S.g_mtl_T + m);
+  return s;
+}
+
 /*******************************************************************************
  * Trace state: one delta-tracking query through the medium
  ******************************************************************************/
@@ -412,6 +475,11 @@ struct Path {
   uint32_t bounces;
   int32_t site_cell, site_layer;
   uint32_t pix, ireal, ri;
+  /* ground: the hit of the walk's last ground query, and the surface the
+   * path leaves (for the self-hit rule) */
+  float3 gN;
+  uint32_t gprim, prev_prim;
+  uint8_t gedge, prev_edge;
 };
 
 /* 32-bit words of a stored path, and of its trace part */
@@ -916,7 +984,15 @@ gen_sample(const DScene& S, const DRequest& R, uint32_t pix, uint32_t ireal)
     for(int i = 0; i < 3; ++i)
       o[i] = R.rect_pos[i] + R.rect_ax[i] * (s0 * 2.0 - 1.0) + R.rect_ay[i] * (s1 * 2.0 - 1.0);
     p.org = mk3((float)o[0], (float)o[1], (float)o[2]);
-    if(S.has_ground && o[2] < 0) {
+    bool inside = S.g_ntris ? false : (S.has_ground && o[2] < 0);
+    if(S.g_ntris) { /* the upward ray must leave through the atmosphere's side */
+      const GHit h = g_trace(S, p.org, make_float3(0.f, 0.f, 1.f), 0.f, FLT_MAX, HG_NO_PRIM, false);
+      if(h.prim != HG_NO_PRIM) {
+        const uint4 f = __ldg(S.g_iface + __ldg(S.g_iface_of + h.prim));
+        inside = (h.ng.z < 0.f ? f.x : f.z) != S.g_sky_mtl; /* cos(up, N) < 0: front */
+      }
+    }
+    if(inside) {
       g.rng = p.rng; g.org = g.rdir = g.dir = p.org; g.flags = PF_REJECTED;
       return g;
     }
@@ -1030,19 +1106,24 @@ struct ScatOut {
  * Out of line: it runs once per scattering and holds the FP64 sun sampling. */
 __device__ __noinline__ ScatOut
 sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float refl,
-           int site_cell, int site_layer, uint32_t band, uint32_t q)
+           int site_cell, int site_layer, uint32_t band, uint32_t q, uint32_t gprim, float3 gN,
+           double wlen_nm)
 {
   ScatOut o;
   const float3 wo = neg3(dir);
   const bool surface = (flags & PF_SURFACE) != 0;
   float3 N = mk3(0.f, 0.f, 1.f);
   bool specular = false;
+  int brdf_specular = 0;
   o.refl = refl;
   o.sdir = mk3(0.f, 0.f, 0.f);
   if(surface) {
+    const SurfProps sp = surface_props(S, rng, dir, gprim, gN, wlen_nm);
+    N = sp.N;
+    brdf_specular = sp.specular;
     if(dot3(N, wo) < 0.f) N = neg3(N);
-    o.refl = S.ground_refl;
-    if(S.ground_brdf == 1) {
+    o.refl = sp.refl;
+    if(sp.specular) {
       o.dnext = nrm3(add3(mul3(N, 2.f * dot3(N, wo)), neg3(wo)));
       specular = true;
     } else {
@@ -1069,7 +1150,7 @@ sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float 
     o.sun_ipdf = (float)S.sun_solid_angle;
     if(surface) {
       const float c = dot3(N, o.sdir);
-      o.R = c < 0.f ? 0.f : (S.ground_brdf == 1 ? 0.f : (c > 0.f ? o.refl / HG_PI_F : 0.f)) * c;
+      o.R = c < 0.f ? 0.f : (brdf_specular ? 0.f : (c > 0.f ? o.refl / HG_PI_F : 0.f)) * c;
     } else {
       const float mu = dot3(dir, o.sdir);
       o.R = (flags & PF_RAYLEIGH) ? rayleigh_eval(mu) : hg_eval(g, mu);
@@ -1098,7 +1179,10 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         if(p.flags & PF_LW) { p.state = ST_LW_WALK; break; }
         p.L_sun = planck_mono(p.wlen_d * 1e-9, S.sun_T);
         if((p.flags & PF_DIRECT) && ((p.flags & PF_IN_CONE) || in_solar_cone(S, p.dir))) {
-          if(ground_trace(S, p.pos, p.dir, 0.f, FLT_MAX, false) < 0.f) {
+          uint32_t hp;
+          bool he;
+          float3 hn;
+          if(ground_query(S, p.pos, p.dir, FLT_MAX, false, 0u, false, &hp, &he, &hn) < 0.f) {
             p.flags |= PF_TRACED;
             trace_begin(p, S, TK_TRANS, HG_KEXT, p.pos, p.dir, 0.f, FLT_MAX, ST_SW_DIRECT_END);
             return;
@@ -1118,7 +1202,12 @@ path_event(Path& p, const DScene& S, const DRequest& R)
 
       case ST_SW_WALK: {
         if(++p.bounces > HG_MAX_BOUNCES) { p.flags |= PF_FAILED; p.state = ST_RAD_END; break; }
-        p.gdist = ground_trace(S, p.pos, p.dir, 0.f, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0);
+        {
+          bool e;
+          p.gdist = ground_query(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
+                                 p.prev_prim, p.prev_edge != 0, &p.gprim, &e, &p.gN);
+          p.gedge = e;
+        }
         p.tr.Ts = p.rng.exp1();
         trace_begin(p, S, TK_SCATTER, HG_KS, p.pos, p.dir, 0.f,
                     p.gdist >= 0.f ? p.gdist : FLT_MAX, ST_SW_SCAT_END);
@@ -1131,8 +1220,13 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         const bool surface = !svx;
         const float tdst = surface ? p.gdist : p.tr.tcur;
         p.pnext = madd3(p.pos, p.dir, tdst);
-        if(surface) p.flags |= PF_SURFACE | PF_PREV_GROUND;
-        else p.flags &= ~(PF_SURFACE | PF_PREV_GROUND);
+        if(surface) {
+          p.flags |= PF_SURFACE | PF_PREV_GROUND;
+          p.prev_prim = p.gprim;
+          p.prev_edge = p.gedge;
+        } else {
+          p.flags &= ~(PF_SURFACE | PF_PREV_GROUND);
+        }
         p.site_cell = p.tr.site_cell;
         p.site_layer = p.tr.site_layer;
         trace_begin(p, S, TK_TRANS, HG_KA, p.pos, p.dir, 0.f, tdst, ST_SW_ABS_END);
@@ -1143,7 +1237,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         p.tr_abs = p.tr.hit ? 0.f : (float)(p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
         if(p.tr_abs <= 0.f) { p.state = ST_RAD_END; break; }
         const ScatOut so = sw_scatter(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
-                                      p.site_layer, p.band, p.q);
+                                      p.site_layer, p.band, p.q, p.gprim, p.gN, p.wlen_d);
         p.rng = so.rng;
         p.flags = so.flags;
         p.dnext = so.dnext;
@@ -1151,8 +1245,12 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         p.R = so.R;
         p.refl = so.refl;
         p.sun_ipdf = so.sun_ipdf;
+        uint32_t hp;
+        bool he;
+        float3 hn;
         if(p.R > 0.f
-        && ground_trace(S, p.pnext, p.sdir, 0.f, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0) < 0.f) {
+        && ground_query(S, p.pnext, p.sdir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0, p.prev_prim,
+                        p.prev_edge != 0, &hp, &he, &hn) < 0.f) {
           p.flags |= PF_TRACED;
           trace_begin(p, S, TK_TRANS, HG_KEXT, p.pnext, p.sdir, 0.f, FLT_MAX, ST_SW_NEE_END);
           return;
@@ -1177,7 +1275,12 @@ path_event(Path& p, const DScene& S, const DRequest& R)
 
       case ST_LW_WALK: {
         if(++p.bounces > HG_MAX_BOUNCES) { p.flags |= PF_FAILED; p.state = ST_RAD_END; break; }
-        p.gdist = ground_trace(S, p.pos, p.dir, 0.f, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0);
+        {
+          bool e;
+          p.gdist = ground_query(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
+                                 p.prev_prim, p.prev_edge != 0, &p.gprim, &e, &p.gN);
+          p.gedge = e;
+        }
         p.tr.Ts = p.rng.exp1();
         trace_begin(p, S, TK_LW, HG_KEXT, p.pos, p.dir, 0.f,
                     p.gdist >= 0.f ? p.gdist : FLT_MAX, ST_LW_END);
@@ -1201,22 +1304,25 @@ path_event(Path& p, const DScene& S, const DRequest& R)
           p.dnext = around(p.dir, hg_mu(p.g, u1), u2);
           p.flags &= ~PF_PREV_GROUND;
         } else {
-          float3 N = mk3(0.f, 0.f, 1.f);
+          const SurfProps sp = surface_props(S, p.rng, p.dir, p.gprim, p.gN, p.wlen_d);
+          float3 N = sp.N;
           const float3 wo = neg3(p.dir);
           if(dot3(N, wo) < 0.f) N = neg3(N);
-          if(S.ground_brdf == 1) {
+          if(sp.specular) {
             p.dnext = nrm3(add3(mul3(N, 2.f * dot3(N, wo)), neg3(wo)));
           } else {
             const float u1 = p.rng.uf(), u2 = p.rng.uf();
             p.dnext = around(N, sqrtf(1.f - u2), u1);
           }
-          if(p.rng.uf() >= S.ground_refl) {
-            const double T = (double)S.ground_T;
+          if(p.rng.uf() >= sp.refl) {
+            const double T = (double)sp.T;
             p.w = T > 0 ? planck_mono(wlen_m, T) : 0.0;
             p.state = ST_RAD_END;
             break;
           }
           p.flags |= PF_PREV_GROUND;
+          p.prev_prim = p.gprim;
+          p.prev_edge = p.gedge;
         }
         p.pos = p.pnext;
         p.dir = p.dnext;

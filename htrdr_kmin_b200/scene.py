@@ -51,6 +51,121 @@ R_EFF = 10e-6  # m
 SIGMA_EXT_CLOUD = 3.0 / (2.0 * RHO_WATER * R_EFF)  # m^2/kg : k_ext = lwc*sigma
 
 
+NO_ID = 0xFFFFFFFF
+
+
+@dataclass
+class GroundMesh:
+    """Ground geometry (htrdr_atmosphere_ground_create,
+    src/atmosphere/htrdr_atmosphere_ground.c:105-160): triangles with an
+    interface each (front, thin, back material; NO_ID: none), materials with a
+    temperature and BRDFs tabulated by wavelength.  A triangle is front-facing
+    on the side from which its vertices are seen clockwise (doc/htrdr-obj.5)."""
+
+    verts: np.ndarray        # float32 [nverts, 3] m
+    tris: np.ndarray         # uint32 [ntris, 3]
+    tri_iface: np.ndarray    # uint32 [ntris]
+    ifaces: np.ndarray       # uint32 [nifaces, 3] front, thin, back
+    mtl_temperature: np.ndarray  # float64 [nmtls] K
+    mtl_nbrdf: np.ndarray    # uint32 [nmtls]
+    mtl_brdf: np.ndarray     # float64 [sum nbrdf, 3] wavelength nm, type (0 Lambertian, 1 specular), reflectivity
+    repeat: bool = False     # repeat the bounding box in X and Y
+    sky_mtl: int = NO_ID     # material of the atmosphere (flux-probe rejection)
+    mtl_names: Tuple[str, ...] = ()
+
+    def fill_desc(self, d, keep: list) -> None:
+        """Set the ground-mesh fields of a ctypes scene description (the CUDA
+        library's or the oracle's: same field names)."""
+        import ctypes as C
+
+        def arr(a, dt, ct):
+            a = np.ascontiguousarray(a, dtype=dt).reshape(-1)
+            keep.append(a)
+            return a.ctypes.data_as(C.POINTER(ct))
+
+        d.ground_nverts = int(self.verts.shape[0])
+        d.ground_verts = arr(self.verts, np.float32, C.c_float)
+        d.ground_ntris = int(self.tris.shape[0])
+        d.ground_tris = arr(self.tris, np.uint32, C.c_uint32)
+        d.ground_tri_iface = arr(self.tri_iface, np.uint32, C.c_uint32)
+        d.ground_nifaces = int(self.ifaces.shape[0])
+        d.ground_ifaces = arr(self.ifaces, np.uint32, C.c_uint32)
+        d.ground_nmtls = int(self.mtl_temperature.shape[0])
+        d.ground_mtl_temperature = arr(self.mtl_temperature, np.float64, C.c_double)
+        d.ground_mtl_nbrdf = arr(self.mtl_nbrdf, np.uint32, C.c_uint32)
+        d.ground_mtl_brdf = arr(self.mtl_brdf if self.mtl_brdf.size else np.zeros((1, 3)), np.float64, C.c_double)
+        d.repeat_ground = int(self.repeat)
+        d.ground_sky_mtl = int(self.sky_mtl)
+
+
+def parse_htrdr_obj(obj_text: str, materials: dict, sky_mtl: str = "air",
+                    repeat: bool = False) -> GroundMesh:
+    """An htrdr-obj ground (doc/htrdr-obj.5): `v x y z`, `f i j k ...`
+    (1-based or negative indices, polygons as fans), `usemtl front:back` or
+    `usemtl front:thin:back`.  `materials' maps a material name to
+    (temperature K, [(wavelength nm, "lambertian"|"specular", reflectivity),
+    ...]) or to None for a semi-transparent material: the htrdr-materials
+    list (doc/htrdr-materials.5) with the tabulated BRDFs given in place of
+    its mrumtl files."""
+    verts, tris, tri_iface = [], [], []
+    iface_ids, ifaces = {}, []
+    names = list(materials.keys())
+    mid = {n: i for i, n in enumerate(names)}
+    cur = None
+    for raw in obj_text.splitlines():
+        line = raw.split("#", 1)[0].strip()
+        if not line:
+            continue
+        tok = line.split()
+        if tok[0] == "v":
+            verts.append([float(tok[1]), float(tok[2]), float(tok[3])])
+        elif tok[0] == "usemtl":
+            parts = " ".join(tok[1:]).split(":")
+            if len(parts) == 2:
+                front, thin, back = parts[0], None, parts[1]
+            elif len(parts) == 3:
+                front, thin, back = parts
+            else:
+                raise ValueError(f"usemtl `{' '.join(tok[1:])}': expected front:back or front:thin:back")
+            key = (front, thin, back)
+            for n in (front, back) + ((thin,) if thin else ()):
+                if n not in mid:
+                    raise ValueError(f"unknown material `{n}'")
+            if key not in iface_ids:
+                iface_ids[key] = len(ifaces)
+                ifaces.append([mid[front], mid[thin] if thin else NO_ID, mid[back]])
+            cur = iface_ids[key]
+        elif tok[0] == "f":
+            if cur is None:
+                raise ValueError("a face outside any usemtl group")
+            ids = []
+            for t in tok[1:]:
+                k = int(t.split("/")[0])
+                ids.append(k - 1 if k > 0 else len(verts) + k)
+            for j in range(1, len(ids) - 1):
+                tris.append([ids[0], ids[j], ids[j + 1]])
+                tri_iface.append(cur)
+    temps, nbrdf, brdf = [], [], []
+    for n in names:
+        m = materials[n]
+        if m is None:
+            temps.append(-1.0)
+            nbrdf.append(0)
+            continue
+        t, table = m
+        temps.append(float(t))
+        nbrdf.append(len(table))
+        for wl, kind, refl in sorted(table):
+            brdf.append([wl, 1.0 if kind == "specular" else 0.0, refl])
+    return GroundMesh(verts=np.array(verts, dtype=np.float32), tris=np.array(tris, dtype=np.uint32),
+                      tri_iface=np.array(tri_iface, dtype=np.uint32),
+                      ifaces=np.array(ifaces, dtype=np.uint32).reshape(-1, 3),
+                      mtl_temperature=np.array(temps, dtype=np.float64),
+                      mtl_nbrdf=np.array(nbrdf, dtype=np.uint32),
+                      mtl_brdf=np.array(brdf, dtype=np.float64).reshape(-1, 3), repeat=repeat,
+                      sky_mtl=mid.get(sky_mtl, NO_ID), mtl_names=tuple(names))
+
+
 @dataclass
 class Scene:
     layer_z: np.ndarray  # float64 [nlayers+1]
@@ -77,6 +192,7 @@ class Scene:
     sun_azimuth: float = 0.0  # deg
     sun_elevation: float = 60.0  # deg
     name: str = "scene"
+    ground_mesh: Optional[GroundMesh] = None  # replaces the plane ground when set
 
     @property
     def nlayers(self) -> int:
@@ -427,4 +543,57 @@ def with_cloud_box(scene: Scene, lwc: np.ndarray, lower, cell, ssa: float, g: fl
     s.cloud_ssa = np.full(scene.nbands, ssa, np.float32)
     s.cloud_g = np.full(scene.nbands, g, np.float32)
     s.repeat_clouds = repeat
+    return s
+
+
+def terrain_materials() -> dict:
+    """Materials of the synthetic terrain: the semi-transparent atmosphere,
+    a Lambertian soil with a tabulated spectral reflectivity and a specular
+    water surface (htrdr-materials list with its BRDF tables inline)."""
+    return {
+        "air": None,
+        "soil": (290.0, [(300.0, "lambertian", 0.08), (550.0, "lambertian", 0.25),
+                         (900.0, "lambertian", 0.40), (8000.0, "lambertian", 0.05)]),
+        "water": (285.0, [(400.0, "specular", 0.06), (10000.0, "specular", 0.02)]),
+    }
+
+
+def terrain_obj(size: float = 3200.0, n: int = 16, amp: float = 150.0, seed: int = SEED_S5,
+                origin=(0.0, 0.0), water_below: float = 0.35) -> str:
+    """An htrdr-obj heightfield over [ox, ox+size] x [oy, oy+size]: n x n
+    quads of two triangles, heights a seeded sum of sines in [0, amp], the
+    quads whose mean height is under `water_below' x amp in the water
+    group, the others soil.  Triangles are clockwise seen from above so the
+    atmosphere is on their front side (`usemtl air:soil')."""
+    rng = np.random.default_rng(seed)
+    k = rng.uniform(1.0, 3.0, size=(3, 2)) * 2.0 * math.pi / size
+    ph = rng.uniform(0.0, 2.0 * math.pi, size=3)
+    xs = origin[0] + np.linspace(0.0, size, n + 1)
+    ys = origin[1] + np.linspace(0.0, size, n + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="xy")
+    H = sum(np.sin(k[i, 0] * X + k[i, 1] * Y + ph[i]) for i in range(3))
+    H = (H - H.min()) / max(float(np.ptp(H)), 1e-9) * amp
+    lines = [f"v {X[j, i]:.3f} {Y[j, i]:.3f} {H[j, i]:.3f}" for j in range(n + 1) for i in range(n + 1)]
+    groups = {"air:soil": [], "air:water": []}
+    for j in range(n):
+        for i in range(n):
+            a = j * (n + 1) + i + 1
+            b, c, d = a + 1, a + (n + 1), a + (n + 1) + 1
+            key = "air:water" if H[j:j + 2, i:i + 2].mean() < water_below * amp else "air:soil"
+            # (a, c, b) and (b, c, d) are clockwise seen from +z
+            groups[key].append(f"f {a} {c} {b}")
+            groups[key].append(f"f {b} {c} {d}")
+    for key, faces in groups.items():
+        if faces:
+            lines.append(f"usemtl {key}")
+            lines.extend(faces)
+    return "\n".join(lines) + "\n"
+
+
+def with_terrain(scene: Scene, size: float = 3200.0, n: int = 16, amp: float = 150.0,
+                 seed: int = SEED_S5, repeat: bool = True) -> Scene:
+    """The scene over the synthetic terrain (replacing its plane ground)."""
+    s = dataclasses.replace(scene)
+    s.ground_mesh = parse_htrdr_obj(terrain_obj(size, n, amp, seed), terrain_materials(),
+                                    sky_mtl="air", repeat=repeat)
     return s

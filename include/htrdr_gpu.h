@@ -87,6 +87,29 @@ struct htrdr_gpu_scene_desc {
   double sun_azimuth, sun_elevation; /* -D, degrees */
   uint32_t props_mask;          /* bit p: build the majorants of property p */
   int32_t octree_on_host;       /* 1: build the octrees on the host CPU (else on the GPU) */
+  /* Ground geometry (htrdr_atmosphere_ground_create,
+   * src/atmosphere/htrdr_atmosphere_ground.c:105-160): a triangle mesh that
+   * replaces the plane ground above when ground_ntris > 0.  A triangle is
+   * front-facing on the side from which its vertices are seen clockwise
+   * (doc/htrdr-obj.5). */
+  uint32_t ground_nverts;
+  const float* ground_verts;        /* [nverts][3] m */
+  uint32_t ground_ntris;
+  const uint32_t* ground_tris;      /* [ntris][3] vertex indices */
+  const uint32_t* ground_tri_iface; /* [ntris] interface of the triangle */
+  uint32_t ground_nifaces;
+  const uint32_t* ground_ifaces;    /* [nifaces][3] front, thin, back material
+                                     * (UINT32_MAX: none; thin is used when set) */
+  uint32_t ground_nmtls;
+  const double* ground_mtl_temperature; /* [nmtls] K (<= 0: no emission) */
+  const uint32_t* ground_mtl_nbrdf;     /* [nmtls] tabulated BRDFs (0: semi-transparent) */
+  const double* ground_mtl_brdf;        /* [sum nbrdf][3]: wavelength nm (ascending per
+                                         * material), type (0 Lambertian, 1 specular),
+                                         * reflectivity */
+  int32_t repeat_ground;            /* repeat the mesh's bounding box infinitely in X and Y */
+  uint32_t ground_sky_mtl;          /* material of the atmosphere: a flux probe whose upward
+                                     * ray meets the mesh from another material is rejected
+                                     * (src/atmosphere/htrdr_atmosphere_draw_map.c:73-99) */
 };
 
 /* One run of the atmosphere command: sensor, spectral domain, output type
@@ -229,6 +252,16 @@ htrdr_gpu_sample_quad(struct htrdr_gpu_scene* scene, size_t n, const double* r,
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_locate_leaf(struct htrdr_gpu_scene* scene, uint32_t iband, uint32_t iquad, int prop,
                       size_t n, const uint32_t* cells, uint32_t* node, uint32_t* level);
+/* Ground ray queries (htrdr_atmosphere_ground_trace_ray,
+ * src/atmosphere/htrdr_atmosphere_ground.c:162-209, with the self-hit filter
+ * of src/core/htrdr_geometry.c:114-150): rays [n] {org[3], dir[3]} (FP32),
+ * range [0, tmax[i]), from_prim[i] the primitive the ray leaves (UINT32_MAX:
+ * none) and from_edge[i] whether that hit lay on an edge.  Out: the hit
+ * primitive (UINT32_MAX: no hit) and distance. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_ground_trace(struct htrdr_gpu_scene* scene, size_t n, const float* rays, const float* tmax,
+                       const uint32_t* from_prim, const uint8_t* from_edge, uint32_t* prim,
+                       float* dist);
 /* Wavelength sampling of a request (htrdr_ran_wlen_planck_sample /
  * htrdr_ran_wlen_cie_xyz_sample_{X,Y,Z}): CDF band index, wavelength, pdf. */
 HTRDR_GPU_API htrdr_gpu_res_T

@@ -78,6 +78,21 @@ struct ora_scene_desc {
   double ground_temperature;
   double sun_azimuth, sun_elevation; /* degrees */
   uint32_t props_mask;        /* bit p: build the octrees of property p */
+  /* ground mesh (replaces the plane when ground_ntris > 0); same arrays as
+   * the CUDA library's scene description */
+  uint32_t ground_nverts;
+  const float* ground_verts;        /* [nverts][3] */
+  uint32_t ground_ntris;
+  const uint32_t* ground_tris;      /* [ntris][3] */
+  const uint32_t* ground_tri_iface; /* [ntris] */
+  uint32_t ground_nifaces;
+  const uint32_t* ground_ifaces;    /* [nifaces][3] front, thin, back (UINT32_MAX: none) */
+  uint32_t ground_nmtls;
+  const double* ground_mtl_temperature; /* [nmtls] */
+  const uint32_t* ground_mtl_nbrdf;     /* [nmtls] */
+  const double* ground_mtl_brdf;        /* [sum nbrdf][3] wavelength nm, type, reflectivity */
+  int32_t repeat_ground;
+  uint32_t ground_sky_mtl;
 };
 
 struct ora_request {
@@ -191,6 +206,13 @@ int ora_draw_map(const struct ora_scene* scn, const struct ora_request* req, voi
 int ora_sample_wavelength(const struct ora_scene* scn, const struct ora_request* req, int channel,
                           size_t n, const double* r0, const double* r1, uint32_t* cdf_band,
                           double* wlen, double* pdf);
+
+/* Ground-mesh queries, one per ray: rays [n][6] (origin, direction), range
+ * [0, tmax), the primitive the ray leaves (UINT32_MAX: none) and whether that
+ * hit lay on an edge.  prim = UINT32_MAX and dist = -1 where nothing is hit. */
+int ora_ground_trace_batch(const struct ora_scene* scn, size_t n, const float* rays,
+                           const float* tmax, const uint32_t* from_prim,
+                           const uint8_t* from_edge, uint32_t* prim, float* dist);
 
 /* Per-realisation weights for pixels [pix_begin, pix_end) (realisation-major
  * inside a pixel): the matched-stream comparison with the GPU. */

@@ -166,7 +166,16 @@ realisation(const struct drv* dv, uint32_t px, uint32_t py, uint32_t ireal, doub
     for(i = 0; i < 3; ++i)
       org[i] = dv->sensor.rpos[i] + dv->sensor.axis_x[i] * (s[0] * 2.0 - 1.0)
              + dv->sensor.axis_y[i] * (s[1] * 2.0 - 1.0);
-    if(scn->has_ground && org[2] < 0) return 0; /* inside the ground: rejected */
+    if(!scn->g_ntris) {
+      if(scn->has_ground && org[2] < 0) return 0; /* inside the ground: rejected */
+    } else { /* the upward ray must leave through the atmosphere's side (:73-99) */
+      const float of[3] = {(float)org[0], (float)org[1], (float)org[2]}, up[3] = {0, 0, 1};
+      const struct ora_ghit h = ora_ground_hit(scn, of, up, 0.f, FLT_MAX, ORA_NO_PRIM, 0);
+      if(h.prim != ORA_NO_PRIM) {
+        const uint32_t* f = scn->g_iface + 3 * (size_t)scn->g_iface_of[h.prim];
+        if((h.ng[2] < 0.f ? f[0] : f[2]) != scn->g_sky_mtl) return 0; /* cos(up, N) < 0: front */
+      }
+    }
     {
       const double u1 = ora_rng_canonical_f(&rng), u2 = ora_rng_canonical_f(&rng);
       double b1[3], b2[3];

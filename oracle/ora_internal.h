@@ -47,6 +47,19 @@ struct ora_scene {
   /* ground */
   int has_ground, ground_brdf;
   double ground_reflectivity, ground_temperature;
+  /* ground mesh (g_ntris > 0 replaces the plane) */
+  uint32_t g_ntris, g_nmtls, g_sky_mtl;
+  int g_repeat;
+  float* g_v;            /* [ntris][3][3] vertices */
+  uint32_t* g_iface_of;  /* [ntris] */
+  uint32_t* g_iface;     /* [nifaces][3] */
+  uint32_t* g_mtl_first; /* [nmtls] */
+  uint32_t* g_mtl_n;     /* [nmtls] */
+  float* g_mtl_T;        /* [nmtls] */
+  double* g_brdf_wl;     /* [nbrdf] */
+  float* g_brdf_type;    /* [nbrdf] */
+  float* g_brdf_refl;    /* [nbrdf] */
+  double g_lower[3], g_upper[3];
   /* sun */
   double sun_dir[3], sun_b1[3], sun_b2[3];
   double sun_cos_half, sun_solid_angle, sun_temperature;
@@ -81,6 +94,23 @@ double ora_site_k(const struct ora_scene* scn, const struct ora_site* s, uint32_
 void ora_onb(const double n[3], double b1[3], double b2[3]);
 double ora_ground_trace(const struct ora_scene* scn, const double o[3], const double d[3],
                         double r0, double r1, int prev_ground);
+
+/* Ground mesh (ora_ground.c) */
+#define ORA_NO_PRIM 0xFFFFFFFFu
+struct ora_ghit {
+  float dist;    /* < 0: none */
+  uint32_t prim;
+  float u, v;
+  float ng[3];   /* (v2 - v0) x (v1 - v0) */
+};
+int ora_ground_setup(struct ora_scene* scn, const struct ora_scene_desc* d);
+void ora_ground_release(struct ora_scene* scn);
+struct ora_ghit ora_ground_hit(const struct ora_scene* scn, const float o[3], const float d[3],
+                               float r0, float r1, uint32_t from_prim, int from_edge);
+int ora_on_edge(float u, float v);
+uint32_t ora_hit_mtl(const struct ora_scene* scn, uint32_t prim, const float ng[3],
+                     const double dir[3]);
+uint32_t ora_fetch_brdf(const struct ora_scene* scn, uint32_t mtl, double wlen, double r);
 
 #ifdef _OPENMP
 #include <omp.h>

@@ -20,6 +20,7 @@
 
 #include <float.h>
 #include <math.h>
+#include <string.h>
 
 /* star-sp ssp_ran_exp(rng, 1) */
 static double
@@ -122,10 +123,10 @@ hemisphere_cos(struct ora_rng* rng, const double N[3], double out[3])
 /* Ground BRDF (htrdr_mtl_create_bsdf, src/core/htrdr_materials.c:414-463):
  * returns the reflectivity; *specular set for the specular BRDF */
 static double
-bsdf_sample(const struct ora_scene* scn, struct ora_rng* rng, const double wo[3],
+bsdf_sample(int brdf_specular, double refl, struct ora_rng* rng, const double wo[3],
             const double N[3], double out[3], int* specular)
 {
-  if(scn->ground_brdf == 1) {
+  if(brdf_specular) {
     const double c = dot3(N, wo);
     int i;
     for(i = 0; i < 3; ++i) out[i] = 2.0 * c * N[i] - wo[i];
@@ -135,14 +136,74 @@ bsdf_sample(const struct ora_scene* scn, struct ora_rng* rng, const double wo[3]
     hemisphere_cos(rng, N, out);
     *specular = 0;
   }
-  return scn->ground_reflectivity;
+  return refl;
 }
 
 static double
-bsdf_eval(const struct ora_scene* scn, const double N[3], const double wi[3])
+bsdf_eval(int brdf_specular, double refl, const double N[3], const double wi[3])
 {
-  if(scn->ground_brdf == 1) return 0.0;
-  return dot3(N, wi) > 0 ? scn->ground_reflectivity / M_PI : 0.0;
+  if(brdf_specular) return 0.0;
+  return dot3(N, wi) > 0 ? refl / M_PI : 0.0;
+}
+
+/* Ground query of the walk: the mesh when the scene has one (FP32 rays, as
+ * the reference converts them for star-3d), else the plane.  `prev': the ray
+ * leaves the ground at (prev_prim, prev_edge).  *h gets the mesh hit. */
+static double
+ground_query(const struct ora_scene* scn, const double o[3], const double d[3], double r1,
+             int prev, uint32_t prev_prim, int prev_edge, struct ora_ghit* h)
+{
+  float of[3], df[3];
+  int i;
+  memset(h, 0, sizeof(*h));
+  h->ng[2] = 1.f;
+  if(!scn->g_ntris) return ora_ground_trace(scn, o, d, 0, r1, prev);
+  for(i = 0; i < 3; ++i) { of[i] = (float)o[i]; df[i] = (float)d[i]; }
+  *h = ora_ground_hit(scn, of, df, 0.f, r1 >= FLT_MAX ? FLT_MAX : (float)r1,
+                      prev ? prev_prim : ORA_NO_PRIM, prev && prev_edge);
+  return h->prim == ORA_NO_PRIM ? -1 : (double)h->dist;
+}
+
+/* Ground properties at a surface event: the normal, the BRDF and the
+ * temperature.  Mesh: the material of the hit side (htrdr_interface_fetch_hit_mtl)
+ * and its BRDF at the wavelength, chosen with one transport canonical
+ * (htrdr_mtl_create_bsdf); a side without a BRDF reflects nothing.  Plane:
+ * its constants, no draw. */
+struct surf {
+  double N[3];
+  double refl, T;
+  int specular;
+};
+
+static struct surf
+surface_props(const struct ora_scene* scn, struct ora_rng* rng, const double dir[3],
+              const struct ora_ghit* h, double wlen)
+{
+  struct surf s;
+  uint32_t m, b;
+  double r, n;
+  if(!scn->g_ntris) {
+    s.N[0] = 0; s.N[1] = 0; s.N[2] = 1;
+    s.refl = scn->ground_reflectivity;
+    s.specular = scn->ground_brdf == 1;
+    s.T = scn->ground_temperature;
+    return s;
+  }
+  n = 1.0 / sqrt((double)h->ng[0] * h->ng[0] + (double)h->ng[1] * h->ng[1] + (double)h->ng[2] * h->ng[2]);
+  s.N[0] = h->ng[0] * n; s.N[1] = h->ng[1] * n; s.N[2] = h->ng[2] * n;
+  m = ora_hit_mtl(scn, h->prim, h->ng, dir);
+  r = canonical(rng);
+  b = m == ORA_NO_PRIM ? ORA_NO_PRIM : ora_fetch_brdf(scn, m, wlen, r);
+  if(b == ORA_NO_PRIM) {
+    s.refl = 0;
+    s.specular = 0;
+    s.T = m == ORA_NO_PRIM ? 0 : scn->g_mtl_T[m];
+    return s;
+  }
+  s.specular = scn->g_brdf_type[b] != 0.f;
+  s.refl = scn->g_brdf_refl[b];
+  s.T = scn->g_mtl_T[m];
+  return s;
 }
 
 /* Sun (src/atmosphere/htrdr_atmosphere_sun.c:126-166) */
@@ -315,12 +376,14 @@ ora_radiance_sw(const struct ora_scene* scn, struct ora_rng* rng, int cpnt_mask,
   const double L_sun = ora_planck_monochromatic(wlen * 1e-9, scn->sun_temperature);
   double pos[3], dir[3], range[2];
   double ksi = 1, w = 0;
-  int prev_ground = 0, i;
+  int prev_ground = 0, prev_edge = 0, i;
+  uint32_t prev_prim = ORA_NO_PRIM;
+  struct ora_ghit gh;
   for(i = 0; i < 3; ++i) { pos[i] = pos_in[i]; dir[i] = dir_in[i]; }
 
   if((cpnt_mask & ORA_DIRECT) && (dir_in_cone || in_solar_cone(scn, dir))) {
     range[0] = 0; range[1] = FLT_MAX;
-    if(ora_ground_trace(scn, pos, dir, range[0], range[1], 0) < 0) {
+    if(ground_query(scn, pos, dir, range[1], 0, 0, 0, &gh) < 0) {
       const double Tr = transmissivity(scn, rng, ORA_KEXT, band, q, pos, dir, range, cnt);
       w = L_sun * Tr;
     }
@@ -333,8 +396,9 @@ ora_radiance_sw(const struct ora_scene* scn, struct ora_rng* rng, int cpnt_mask,
     double pos_next[3], dir_next[3], wo[3], N[3] = {0, 0, 1}, sun_dir[3];
     double ground_dst, Tr_abs, Tr, R, sun_pdf, refl = 1;
     int surface, svx_hit, specular = 0, phase = PHASE_HG;
+    struct surf sp = {{0, 0, 1}, 0, 0, 0};
 
-    ground_dst = ora_ground_trace(scn, pos, dir, 0, DBL_MAX, prev_ground);
+    ground_dst = ground_query(scn, pos, dir, DBL_MAX, prev_ground, prev_prim, prev_edge, &gh);
 
     sc.scn = scn; sc.rng = rng; sc.band = band; sc.q = q; sc.prop = ORA_KS; sc.cnt = cnt;
     sc.Ts = ran_exp(rng);
@@ -349,14 +413,17 @@ ora_radiance_sw(const struct ora_scene* scn, struct ora_rng* rng, int cpnt_mask,
     if(surface) sc.traversal_dst = ground_dst;
     for(i = 0; i < 3; ++i) pos_next[i] = pos[i] + dir[i] * sc.traversal_dst;
     prev_ground = surface;
+    if(surface) { prev_prim = gh.prim; prev_edge = ora_on_edge(gh.u, gh.v) && scn->g_ntris; }
 
     range[0] = 0; range[1] = sc.traversal_dst;
     Tr_abs = transmissivity(scn, rng, ORA_KA, band, q, pos, dir, range, cnt);
     if(Tr_abs <= 0) break;
 
     if(surface) {
+      sp = surface_props(scn, rng, dir, &gh, wlen);
+      N[0] = sp.N[0]; N[1] = sp.N[1]; N[2] = sp.N[2];
       if(dot3(N, wo) < 0) { N[0] = -N[0]; N[1] = -N[1]; N[2] = -N[2]; }
-      refl = bsdf_sample(scn, rng, wo, N, dir_next, &specular);
+      refl = bsdf_sample(sp.specular, sp.refl, rng, wo, N, dir_next, &specular);
     } else {
       const double ks_gas = ora_site_k(scn, &sc.site, band, q, ORA_KS, 1);
       const double ks_par = ora_site_k(scn, &sc.site, band, q, ORA_KS, 2);
@@ -376,7 +443,7 @@ ora_radiance_sw(const struct ora_scene* scn, struct ora_rng* rng, int cpnt_mask,
     } else {
       sun_pdf = sun_sample(scn, rng, sun_dir);
       if(surface) {
-        R = dot3(N, sun_dir) < 0 ? 0 : bsdf_eval(scn, N, sun_dir) * dot3(N, sun_dir);
+        R = dot3(N, sun_dir) < 0 ? 0 : bsdf_eval(sp.specular, sp.refl, N, sun_dir) * dot3(N, sun_dir);
       } else {
         R = phase_eval(phase, g, wo, sun_dir);
       }
@@ -386,7 +453,8 @@ ora_radiance_sw(const struct ora_scene* scn, struct ora_rng* rng, int cpnt_mask,
       Tr = 0;
     } else {
       range[0] = 0; range[1] = FLT_MAX;
-      if(ora_ground_trace(scn, pos_next, sun_dir, range[0], range[1], prev_ground) >= 0) Tr = 0;
+      struct ora_ghit sh;
+      if(ground_query(scn, pos_next, sun_dir, range[1], prev_ground, prev_prim, prev_edge, &sh) >= 0) Tr = 0;
       else Tr = transmissivity(scn, rng, ORA_KEXT, band, q, pos_next, sun_dir, range, cnt);
     }
 
@@ -413,14 +481,17 @@ ora_radiance_lw(const struct ora_scene* scn, struct ora_rng* rng, const double p
   const double g = (double)scn->cloud_g[iband];
   const double wlen_m = wlen * 1e-9;
   double pos[3], dir[3], range[2], w = 0;
-  int prev_ground = 0, i;
+  int prev_ground = 0, prev_edge = 0, i;
+  uint32_t prev_prim = ORA_NO_PRIM;
   for(i = 0; i < 3; ++i) { pos[i] = pos_in[i]; dir[i] = dir_in[i]; }
 
   for(;;) {
     struct sctx c;
     struct ora_seg hit;
+    struct ora_ghit gh;
     double pos_next[3], dir_next[3], wo[3];
-    const double ground_dst = ora_ground_trace(scn, pos, dir, 0, DBL_MAX, prev_ground);
+    const double ground_dst = ground_query(scn, pos, dir, DBL_MAX, prev_ground, prev_prim, prev_edge,
+                                           &gh);
     int svx_hit;
 
     c.scn = scn; c.rng = rng; c.band = band; c.q = q; c.prop = ORA_KEXT; c.cnt = cnt;
@@ -443,17 +514,21 @@ ora_radiance_lw(const struct ora_scene* scn, struct ora_rng* rng, const double p
       phase_sample(PHASE_HG, g, rng, dir, dir_next);
       prev_ground = 0;
     } else { /* surface */
-      double N[3] = {0, 0, 1};
+      const struct surf sp = surface_props(scn, rng, dir, &gh, wlen);
+      double N[3];
       int specular;
       double refl;
+      N[0] = sp.N[0]; N[1] = sp.N[1]; N[2] = sp.N[2];
       if(dot3(N, wo) < 0) { N[0] = -N[0]; N[1] = -N[1]; N[2] = -N[2]; }
-      refl = bsdf_sample(scn, rng, wo, N, dir_next, &specular);
+      refl = bsdf_sample(sp.specular, sp.refl, rng, wo, N, dir_next, &specular);
       if(canonical(rng) >= refl) {
-        const double T = scn->ground_temperature;
+        const double T = sp.T;
         w = T > 0 ? ora_planck_monochromatic(wlen_m, T) : 0;
         break;
       }
       prev_ground = 1;
+      prev_prim = gh.prim;
+      prev_edge = scn->g_ntris && ora_on_edge(gh.u, gh.v);
     }
     for(i = 0; i < 3; ++i) { pos[i] = pos_next[i]; dir[i] = dir_next[i]; }
   }

@@ -430,6 +430,7 @@ ora_scene_create(const struct ora_scene_desc* d, struct ora_scene** out)
   s->ground_brdf = d->ground_brdf;
   s->ground_reflectivity = d->ground_reflectivity;
   s->ground_temperature = d->ground_temperature;
+  if(ora_ground_setup(s, d)) { ora_scene_release(s); return ORA_RES_MEM_ERR; }
   { /* Sun (src/atmosphere/htrdr_atmosphere_sun.c:66-101, htrdr_atmosphere.c:360-364) */
     const double az = d->sun_azimuth * M_PI / 180.0, el = d->sun_elevation * M_PI / 180.0;
     s->sun_dir[0] = cos(el) * cos(az);
@@ -457,6 +458,7 @@ ora_scene_release(struct ora_scene* s)
   free(s->nquads); free(s->quad_off); free(s->quad_cum); free(s->gas_ka); free(s->gas_ks);
   free(s->gas_kext); free(s->sig); free(s->cloud_g); free(s->lwc);
   free(s->cell_layer_lo); free(s->cell_layer_hi);
+  ora_ground_release(s);
   free(s);
 }
 

@@ -50,6 +50,13 @@ class SceneDesc(C.Structure):
         ("ground_reflectivity", C.c_double), ("ground_temperature", C.c_double),
         ("sun_azimuth", C.c_double), ("sun_elevation", C.c_double),
         ("props_mask", C.c_uint32),
+        ("ground_nverts", C.c_uint32), ("ground_verts", C.POINTER(C.c_float)),
+        ("ground_ntris", C.c_uint32), ("ground_tris", C.POINTER(C.c_uint32)),
+        ("ground_tri_iface", C.POINTER(C.c_uint32)), ("ground_nifaces", C.c_uint32),
+        ("ground_ifaces", C.POINTER(C.c_uint32)), ("ground_nmtls", C.c_uint32),
+        ("ground_mtl_temperature", C.POINTER(C.c_double)),
+        ("ground_mtl_nbrdf", C.POINTER(C.c_uint32)), ("ground_mtl_brdf", C.POINTER(C.c_double)),
+        ("repeat_ground", C.c_int32), ("ground_sky_mtl", C.c_uint32),
     ]
 
 
@@ -123,6 +130,10 @@ def lib() -> C.CDLL:
                                             C.c_size_t, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double), C.POINTER(C.c_uint32),
                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ora_ground_trace_batch.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_float),
+                                             C.POINTER(C.c_float), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint8), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_float)]
         for name in ("ora_wiebelt",):
             getattr(L, name).argtypes = [C.c_double]
             getattr(L, name).restype = C.c_double
@@ -189,6 +200,8 @@ class OracleScene:
         d.sun_azimuth = scene.sun_azimuth
         d.sun_elevation = scene.sun_elevation
         d.props_mask = props_mask
+        if scene.ground_mesh is not None:
+            scene.ground_mesh.fill_desc(d, keep)
         h = C.c_void_p()
         res = lib().ora_scene_create(C.byref(d), C.byref(h))
         if res != 0:
@@ -267,6 +280,22 @@ class OracleScene:
         if res != 0:
             raise RuntimeError(res)
         return out
+
+    def ground_trace(self, rays, tmax, from_prim, from_edge):
+        """Ground-mesh queries (ora_ground.c): (primitive, distance) per ray."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        fp = np.ascontiguousarray(from_prim, np.uint32)
+        fe = np.ascontiguousarray(from_edge, np.uint8)
+        n = rays.shape[0]
+        prim = np.zeros(n, np.uint32)
+        dist = np.zeros(n, np.float32)
+        res = lib().ora_ground_trace_batch(self.handle, n, _p(rays, C.c_float), _p(tmax, C.c_float),
+                                           _p(fp, C.c_uint32), _p(fe, C.c_uint8),
+                                           _p(prim, C.c_uint32), _p(dist, C.c_float))
+        if res != 0:
+            raise RuntimeError(f"ora_ground_trace_batch failed: {res}")
+        return prim, dist
 
     def radiance(self, lw: bool, pos, dirs, wlen, iband, iquad, mask: int = ALL,
                  seed: int = 0, nthreads: int = 0) -> np.ndarray:

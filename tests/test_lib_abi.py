@@ -82,3 +82,31 @@ def test_tuning_struct_and_engine_fields():
     assert t.engine == api.ENGINE_PERSISTENT and t.wave_slots == 0 and t.trace_budget == 0
     for mode in (S.MODE_XWAVE_SW, S.MODE_XWAVE_LW, S.MODE_IMAGE_CIE, S.MODE_FLUX_SW, S.MODE_FLUX_LW):
         assert api.mode_tuning(mode).engine in (api.ENGINE_PERSISTENT, api.ENGINE_WAVEFRONT)
+
+
+@pytest.mark.parametrize("struct,mirror", [
+    ("htrdr_gpu_scene_desc", "SceneDesc"), ("htrdr_gpu_request", "Request"),
+    ("htrdr_gpu_buffer_layout", "BufferLayout"), ("htrdr_gpu_stats", "Stats"),
+    ("htrdr_gpu_map_summary", "MapSummary"), ("htrdr_gpu_batch_item", "BatchItem"),
+    ("htrdr_gpu_tuning", "Tuning"), ("htrdr_gpu_server_config", "ServerConfig"),
+    ("htrdr_gpu_server_stats", "ServerStats")])
+def test_struct_layout_matches_header(tmp_path, struct, mirror):
+    """Every field of the ctypes mirror sits at the C struct's offset."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    cls = getattr(api, mirror)
+    names = [f[0] for f in cls._fields_]
+    src = ["#include <stddef.h>", "#include <stdio.h>", '#include "htrdr_gpu.h"', "int main(void) {",
+           f'  printf("%zu\\n", sizeof(struct {struct}));']
+    src += [f'  printf("%zu\\n", offsetof(struct {struct}, {n}));' for n in names]
+    src += ["  return 0;", "}"]
+    (tmp_path / "l.c").write_text("\n".join(src))
+    exe = tmp_path / "l"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(tmp_path / "l.c"), "-o", str(exe)],
+                   check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert out[0] == C.sizeof(cls)
+    assert out[1:] == [getattr(cls, n).offset for n in names]
