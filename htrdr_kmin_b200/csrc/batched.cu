@@ -29,6 +29,7 @@
 
 namespace hg {
 
+template <bool MESH>
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
 k_persistent(PTables T, int tables_in_smem)
 {
@@ -75,7 +76,7 @@ k_persistent(PTables T, int tables_in_smem)
       const DRequest& R = T.reqs[p.ri];
       const DScene& S = T.scenes[p.si];
       if(p.state != ST_TRACE && p.state != ST_DONE) {
-        path_event(p, S, R);
+        path_event<MESH>(p, S, R);
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
         p.c_seg = p.c_node = p.c_tc = 0;
       }
@@ -111,17 +112,18 @@ launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
   const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
   const int in_smem = tables <= 96 * 1024;
   const size_t smem = in_smem ? tables : 0;
+  auto kern = T.has_mesh ? k_persistent<true> : k_persistent<false>;
   if(smem > 48 * 1024) {
-    const cudaError_t e = cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
     if(e != cudaSuccess) return e;
   }
   int nsm = 0, per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)block_size, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)block_size, smem);
   if(blocks_per_sm) per_sm = std::min(per_sm, (int)blocks_per_sm);
   per_sm = std::max(per_sm, 1);
-  k_persistent<<<(unsigned)(nsm * per_sm), block_size, smem, st>>>(T, in_smem);
+  kern<<<(unsigned)(nsm * per_sm), block_size, smem, st>>>(T, in_smem);
   note_launches(1);
   return cudaGetLastError();
 }
@@ -173,6 +175,7 @@ launch_workqueue_single(const DScene& S, const DRequest& R, void* tables, void* 
   T.items = &d->item;
   T.offsets = d->offsets;
   T.nscenes = 1;
+  T.has_mesh = S.g_ntris != 0;
   T.nreqs = 1;
   T.nitems = 1;
   T.total = h.offsets[1];
@@ -187,7 +190,7 @@ persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device)
 {
   int nsm = 0, per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, (int)block_size, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<true>, (int)block_size, 0);
   if(blocks_per_sm) per_sm = std::min(per_sm, (int)blocks_per_sm);
   return (uint64_t)std::max(per_sm, 1) * (uint64_t)nsm * block_size;
 }
@@ -270,6 +273,7 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
   T.items = (const PItem*)P.d_items.ptr;
   T.offsets = (const uint64_t*)P.d_offsets.ptr;
   T.nscenes = (uint32_t)P.scenes.size();
+  T.has_mesh = std::any_of(P.scenes.begin(), P.scenes.end(), [](const DScene& d) { return d.g_ntris != 0; });
   T.nreqs = (uint32_t)n;
   T.nitems = (uint32_t)n;
   T.total = P.offsets[n];

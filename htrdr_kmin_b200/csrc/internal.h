@@ -151,6 +151,7 @@ struct PTables {
   unsigned long long* next; /* queue head (zeroed before the launch) */
   void* cnt;                /* Counters (zeroed before the launch) */
   uint32_t chunk, regroup_period;
+  uint32_t has_mesh;        /* some scene has a ground mesh (selects the kernels' variant) */
 };
 cudaError_t launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
                               int device, cudaStream_t st);

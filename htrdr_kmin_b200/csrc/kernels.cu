@@ -9,13 +9,14 @@
 
 namespace hg {
 
+template <bool MESH>
 __device__ __forceinline__ void
 run_path(Path& p, const DScene& S, const DRequest& R)
 {
   for(;;) {
     if(p.state == ST_TRACE) trace_step(p, S);
     else if(p.state == ST_DONE) return;
-    else path_event(p, S, R);
+    else path_event<MESH>(p, S, R);
   }
 }
 
@@ -58,6 +59,7 @@ flush_counters(Counters* cnt, unsigned long long seg, unsigned long long node,
   }
 }
 
+template <bool MESH>
 __global__ void __maxnreg__(HG_PLAIN_MAXNREG)
 k_plain(DScene S, DRequest R, DAccum* acc, DAccum* tacc, uint64_t pix_begin, uint32_t npix,
         double* weights, Counters* cnt)
@@ -71,7 +73,7 @@ k_plain(DScene S, DRequest R, DAccum* acc, DAccum* tacc, uint64_t pix_begin, uin
     p.pix = (uint32_t)(pix_begin + idx % npix);
     p.state = ST_GEN;
     p.flags = 0;
-    run_path(p, S, R);
+    run_path<MESH>(p, S, R);
     if(weights) {
       weights[(idx % npix) * R.nreal_pp + p.ireal] =
         (p.flags & (PF_REJECTED | PF_FAILED)) ? __longlong_as_double(0x7ff8000000000000ll) : p.weight;
@@ -164,6 +166,7 @@ k_finalize(DRequest R, const DAccum* acc, const DAccum* tacc, char* out, size_t 
 /*******************************************************************************
  * Batched radiance (atmosphere_compute_radiance_sw/_lw with one stream per ray)
  ******************************************************************************/
+template <bool MESH>
 __global__ void __launch_bounds__(128)
 k_radiance(DScene S, int lw, size_t n, const double* pos, const double* dir, const double* wlen,
            const uint32_t* band, const uint32_t* iquad, int mask, uint32_t seed, double* out)
@@ -186,7 +189,7 @@ k_radiance(DScene S, int lw, size_t n, const double* pos, const double* dir, con
   p.flags = lw ? PF_LW : (((mask & 1) ? PF_DIRECT : 0u) | ((mask & 2) ? PF_DIFFUSE : 0u));
   p.c_seg = p.c_node = p.c_tc = 0;
   p.state = ST_RAD_BEGIN;
-  run_path(p, S, R);
+  run_path<MESH>(p, S, R);
   out[i] = (p.flags & PF_FAILED) ? __longlong_as_double(0x7ff8000000000000ll) : p.weight;
 }
 
@@ -269,8 +272,9 @@ launch_plain(const DScene& S, const DRequest& R, DAccum* acc, DAccum* tacc, uint
   DRequest Ra = R;
   Ra.acc = acc;
   Ra.tacc = tacc;
-  k_plain<<<nblocks(total, 128), 128, 0, st>>>(S, Ra, acc, tacc, pix_begin, npix, weights,
-                                               (Counters*)counters);
+  auto kern = S.g_ntris ? k_plain<true> : k_plain<false>;
+  kern<<<nblocks(total, 128), 128, 0, st>>>(S, Ra, acc, tacc, pix_begin, npix, weights,
+                                            (Counters*)counters);
   note_launches(1);
   return cudaGetLastError();
 }
@@ -294,7 +298,8 @@ launch_radiance(const DScene& S, int lw, size_t n, const double* pos, const doub
                 uint32_t seed, double* out, cudaStream_t st)
 {
   if(!n) return cudaSuccess;
-  k_radiance<<<nblocks(n, 128), 128, 0, st>>>(S, lw, n, pos, dir, wlen, band, iquad, mask, seed, out);
+  auto kern = S.g_ntris ? k_radiance<true> : k_radiance<false>;
+  kern<<<nblocks(n, 128), 128, 0, st>>>(S, lw, n, pos, dir, wlen, band, iquad, mask, seed, out);
   return cudaGetLastError();
 }
 

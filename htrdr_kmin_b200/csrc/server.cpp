@@ -215,6 +215,7 @@ htrdr_gpu_server::launch_round(Slot& s, const std::vector<SReq*>& act)
   T.items = (const PItem*)s.items.ptr;
   T.offsets = (const uint64_t*)s.offsets.ptr;
   T.nscenes = (uint32_t)scenes.size();
+  T.has_mesh = std::any_of(scenes.begin(), scenes.end(), [](const DScene& d) { return d.g_ntris != 0; });
   T.nreqs = (uint32_t)reqs.size();
   T.nitems = (uint32_t)items.size();
   T.total = offsets.back();
@@ -482,6 +483,8 @@ htrdr_gpu_server::wave_tables_now()
   T.items = (const PItem*)w_items.ptr;
   T.offsets = (const uint64_t*)w_offsets.ptr;
   T.nscenes = (uint32_t)w_scene_of.size();
+  T.has_mesh = std::any_of(w_scene_of.begin(), w_scene_of.end(),
+                           [](const htrdr_gpu_scene* sc) { return sc && sc->d.g_ntris != 0; });
   T.nreqs = w_nreqs;
   T.nitems = (uint32_t)w_nitems;
   T.total = w_appended;

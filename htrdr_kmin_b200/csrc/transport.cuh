@@ -351,11 +351,12 @@ ground_trace(const DScene& S, float3 o, float3 d, float r0, float r1, bool prev_
  * plane: distance in [0, r1) (< 0: none), the hit primitive, whether the hit
  * lies on an edge and the geometric normal.  `prev' says the ray leaves the
  * ground at (prev_prim, prev_edge). */
+template <bool MESH>
 __device__ __forceinline__ float
 ground_query(const DScene& S, float3 o, float3 d, float r1, bool prev, uint32_t prev_prim,
              bool prev_edge, uint32_t* prim, bool* edge, float3* ng)
 {
-  if(!S.g_ntris) {
+  if(!MESH || !S.g_ntris) {
     *prim = 0;
     *edge = false;
     *ng = make_float3(0.f, 0.f, 1.f);
@@ -380,11 +381,12 @@ struct SurfProps {
   int specular;
 };
 
+template <bool MESH>
 __device__ __forceinline__ SurfProps
 surface_props(const DScene& S, Rng& rng, float3 dir, uint32_t prim, float3 ng, double wlen_nm)
 {
   SurfProps s;
-  if(!S.g_ntris) {
+  if(!MESH || !S.g_ntris) {
     s.N = make_float3(0.f, 0.f, 1.f);
     s.refl = S.ground_refl;
     s.specular = S.ground_brdf == 1;
@@ -1104,6 +1106,7 @@ struct ScatOut {
  * the next-event estimate with its phase/BRDF value
  * (htrdr_atmosphere_compute_radiance_sw.c:400-490).
  * Out of line: it runs once per scattering and holds the FP64 sun sampling. */
+template <bool MESH>
 __device__ __noinline__ ScatOut
 sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float refl,
            int site_cell, int site_layer, uint32_t band, uint32_t q, uint32_t gprim, float3 gN,
@@ -1118,7 +1121,7 @@ sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float 
   o.refl = refl;
   o.sdir = mk3(0.f, 0.f, 0.f);
   if(surface) {
-    const SurfProps sp = surface_props(S, rng, dir, gprim, gN, wlen_nm);
+    const SurfProps sp = surface_props<MESH>(S, rng, dir, gprim, gN, wlen_nm);
     N = sp.N;
     brdf_specular = sp.specular;
     if(dot3(N, wo) < 0.f) N = neg3(N);
@@ -1162,7 +1165,9 @@ sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float 
 }
 
 /* Advance the state machine until the path needs a voxel step (ST_TRACE),
- * is done (ST_DONE) or idle. */
+ * is done (ST_DONE) or idle.  MESH = false: the scenes of the launch have
+ * the plane ground only (the mesh queries are compiled out). */
+template <bool MESH>
 __device__ __forceinline__ void
 path_event(Path& p, const DScene& S, const DRequest& R)
 {
@@ -1182,7 +1187,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
           uint32_t hp;
           bool he;
           float3 hn;
-          if(ground_query(S, p.pos, p.dir, FLT_MAX, false, 0u, false, &hp, &he, &hn) < 0.f) {
+          if(ground_query<MESH>(S, p.pos, p.dir, FLT_MAX, false, 0u, false, &hp, &he, &hn) < 0.f) {
             p.flags |= PF_TRACED;
             trace_begin(p, S, TK_TRANS, HG_KEXT, p.pos, p.dir, 0.f, FLT_MAX, ST_SW_DIRECT_END);
             return;
@@ -1204,7 +1209,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         if(++p.bounces > HG_MAX_BOUNCES) { p.flags |= PF_FAILED; p.state = ST_RAD_END; break; }
         {
           bool e;
-          p.gdist = ground_query(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
+          p.gdist = ground_query<MESH>(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
                                  p.prev_prim, p.prev_edge != 0, &p.gprim, &e, &p.gN);
           p.gedge = e;
         }
@@ -1236,7 +1241,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
       case ST_SW_ABS_END: {
         p.tr_abs = p.tr.hit ? 0.f : (float)(p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
         if(p.tr_abs <= 0.f) { p.state = ST_RAD_END; break; }
-        const ScatOut so = sw_scatter(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
+        const ScatOut so = sw_scatter<MESH>(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
                                       p.site_layer, p.band, p.q, p.gprim, p.gN, p.wlen_d);
         p.rng = so.rng;
         p.flags = so.flags;
@@ -1249,7 +1254,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         bool he;
         float3 hn;
         if(p.R > 0.f
-        && ground_query(S, p.pnext, p.sdir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0, p.prev_prim,
+        && ground_query<MESH>(S, p.pnext, p.sdir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0, p.prev_prim,
                         p.prev_edge != 0, &hp, &he, &hn) < 0.f) {
           p.flags |= PF_TRACED;
           trace_begin(p, S, TK_TRANS, HG_KEXT, p.pnext, p.sdir, 0.f, FLT_MAX, ST_SW_NEE_END);
@@ -1277,7 +1282,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         if(++p.bounces > HG_MAX_BOUNCES) { p.flags |= PF_FAILED; p.state = ST_RAD_END; break; }
         {
           bool e;
-          p.gdist = ground_query(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
+          p.gdist = ground_query<MESH>(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
                                  p.prev_prim, p.prev_edge != 0, &p.gprim, &e, &p.gN);
           p.gedge = e;
         }
@@ -1304,7 +1309,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
           p.dnext = around(p.dir, hg_mu(p.g, u1), u2);
           p.flags &= ~PF_PREV_GROUND;
         } else {
-          const SurfProps sp = surface_props(S, p.rng, p.dir, p.gprim, p.gN, p.wlen_d);
+          const SurfProps sp = surface_props<MESH>(S, p.rng, p.dir, p.gprim, p.gN, p.wlen_d);
           float3 N = sp.N;
           const float3 wo = neg3(p.dir);
           if(dot3(N, wo) < 0.f) N = neg3(N);

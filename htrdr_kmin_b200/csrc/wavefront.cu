@@ -93,6 +93,7 @@ struct WTables {
 
 /* Iteration parity b: the event stage reads list b and writes list b^1; the
  * trace stage then walks list b^1. */
+template <bool MESH>
 __global__ void __launch_bounds__(128)
 k_wave_event(WTables W, uint32_t b, int tables_in_smem)
 {
@@ -145,7 +146,7 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
       if(!__any_sync(0xffffffffu, busy)) break;
       if(busy) {
         if(p.state != ST_DONE) {
-          path_event(p, T.scenes[p.si], T.reqs[p.ri]);
+          path_event<MESH>(p, T.scenes[p.si], T.reqs[p.ri]);
           seg += p.c_seg; node += p.c_node; tc += p.c_tc;
           p.c_seg = p.c_node = p.c_tc = 0;
         }
@@ -301,6 +302,7 @@ k_wave_clamp(WTables W)
  * live list 0 from their slots, then take any realisations left in the work
  * queue; events and traces run in the same thread, events regrouped every
  * `regroup_period' voxel steps as in the persistent engine. */
+template <bool MESH>
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
 k_wave_finish(WTables W, int tables_in_smem)
 {
@@ -363,7 +365,7 @@ k_wave_finish(WTables W, int tables_in_smem)
       const DRequest& R = T.reqs[p.ri];
       const DScene& S = T.scenes[p.si];
       if(p.state != ST_TRACE && p.state != ST_DONE) {
-        path_event(p, S, R);
+        path_event<MESH>(p, S, R);
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
         p.c_seg = p.c_node = p.c_tc = 0;
       }
@@ -436,6 +438,10 @@ struct WaveLaunch {
   unsigned ev_grid = 0, tr_grid = 0, fi_grid = 0;
   uint32_t tb = 256;
   uint64_t tail = 0;  /* live paths below which the rest finishes in the megakernel */
+  /* the event and tail kernels of the tables' scenes (with or without the
+   * ground-mesh queries) */
+  void (*ev)(WTables, uint32_t, int) = nullptr;
+  void (*fi)(WTables, int) = nullptr;
 };
 
 cudaError_t
@@ -444,21 +450,23 @@ wave_params(const PTables& T, const htrdr_gpu_tuning& tun, int device, WaveLaunc
   const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
   L.in_smem = tables <= 96 * 1024;
   L.smem = L.in_smem ? tables : 0;
+  L.ev = T.has_mesh ? k_wave_event<true> : k_wave_event<false>;
+  L.fi = T.has_mesh ? k_wave_finish<true> : k_wave_finish<false>;
   cudaError_t e;
   if(L.smem > 48 * 1024) {
-    if((e = cudaFuncSetAttribute(k_wave_event, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
+    if((e = cudaFuncSetAttribute(L.ev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
       return e;
     if((e = cudaFuncSetAttribute(k_wave_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
       return e;
-    if((e = cudaFuncSetAttribute(k_wave_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
+    if((e = cudaFuncSetAttribute(L.fi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
       return e;
   }
   int nsm = 0, ev_per_sm = 0, tr_per_sm = 0, fi_per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   L.tb = tun.block_size ? tun.block_size : 256;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ev_per_sm, k_wave_event, 128, L.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ev_per_sm, L.ev, 128, L.smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, k_wave_trace, (int)L.tb, L.smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, k_wave_finish, (int)L.tb, L.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, L.fi, (int)L.tb, L.smem);
   if(tun.blocks_per_sm) tr_per_sm = std::min(tr_per_sm, (int)tun.blocks_per_sm);
   L.ev_grid = (unsigned)(nsm * std::max(ev_per_sm, 1));
   L.tr_grid = (unsigned)(nsm * std::max(tr_per_sm, 1));
@@ -488,7 +496,7 @@ wave_iterations(const WTables& W, const WaveLaunch& L, uint32_t C, cudaStream_t 
 {
   for(uint32_t i = 0; i < C; ++i) {
     const uint32_t b = i & 1u;
-    k_wave_event<<<L.ev_grid, 128, L.smem, st>>>(W, b, L.in_smem);
+    L.ev<<<L.ev_grid, 128, L.smem, st>>>(W, b, L.in_smem);
     k_wave_trace<<<L.tr_grid, L.tb, L.smem, st>>>(W, b, L.in_smem);
   }
   note_launches(2 * C);
@@ -514,7 +522,7 @@ launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int
    * whole queue */
   if(P < L.tail) {
     k_wave_init<<<1, 32, 0, st>>>(W, 0u);
-    k_wave_finish<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+    L.fi<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
     note_launches(2);
     return cudaGetLastError();
   }
@@ -542,7 +550,7 @@ launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int
       const uint32_t live = hctl[(k - 1) & 1].n_live[0];
       if(live == 0) break;  /* chunk k runs empty stages */
       if(live < L.tail) {   /* after chunk k, the megakernel finishes list 0 */
-        k_wave_finish<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+        L.fi<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
         note_launches(1);
         return cudaGetLastError();
       }
@@ -601,7 +609,7 @@ wave_serve_finish(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, in
   cudaError_t e = wave_params(T, tun, device, L);
   if(e) return e;
   const WTables W = wave_tables(T, tun, B, true);
-  k_wave_finish<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+  L.fi<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
   k_wave_clamp<<<1, 32, 0, st>>>(W);
   note_launches(2);
   if((e = cudaGetLastError())) return e;

@@ -154,3 +154,34 @@ def test_terrain_engines_agree(gpu_lib):
     a = out[gpu_lib.ENGINE_PLAIN]["L"]
     for eng in (gpu_lib.ENGINE_PERSISTENT, gpu_lib.ENGINE_WAVEFRONT):
         np.testing.assert_allclose(out[eng]["L"], a, rtol=1e-9, atol=0)
+
+
+def test_terrain_in_batches(gpu_lib):
+    """A batch that mixes a terrain scene with plane-ground scenes runs the
+    mesh variant of the batched kernels and equals each map drawn alone on
+    the plain engine, on the persistent and on the wavefront engine."""
+    sc1, rq1 = S.config_c1(scale=10 / 64, spp=8)
+    sc1 = S.with_terrain(sc1)
+    rq1.cam_pos, rq1.cam_tgt, rq1.cam_up = (1600.0, -600.0, 700.0), (1600.0, 1600.0, 0.0), (0, 0, 1)
+    sc2, rq2 = S.config_c1(scale=8 / 64, spp=8)
+    sc3, rq3 = S.config_c2(scale=8 / 128, spp=16, cloud_def=(16, 16, 8))
+    sc3 = S.with_terrain(sc3)
+    rq3.rect_pos, rq3.rect_tgt = (800.0, 800.0, 75.0), (800.0, 800.0, 76.0)
+    items = [(gpu_lib.GpuScene(sc1, 0b111), rq1), (gpu_lib.GpuScene(sc2, 0b111), rq2),
+             (gpu_lib.GpuScene(sc3, 0b100), rq3)]
+    alone = []
+    for gs, rq in items:
+        gs.set_engine(gpu_lib.ENGINE_PLAIN)
+        alone.append(gs.draw_map(rq)[0])
+    for eng in (gpu_lib.ENGINE_PERSISTENT, gpu_lib.ENGINE_WAVEFRONT):
+        t = gpu_lib.default_tuning()
+        t.engine = eng
+        if eng == gpu_lib.ENGINE_WAVEFRONT:
+            t.wave_tail, t.regroup_period, t.trace_budget = 100, 16, 64
+        bufs, st = gpu_lib.draw_maps_batched(items, t)
+        for b, a, (_, rq) in zip(bufs, alone, items):
+            if rq.mode in (S.MODE_FLUX_SW, S.MODE_FLUX_LW):
+                np.testing.assert_array_equal(b["n"], a["n"])
+                np.testing.assert_allclose(b["sum"], a["sum"], rtol=1e-9, atol=0)
+            else:
+                np.testing.assert_allclose(b["L"], a["L"], rtol=1e-9, atol=0)
