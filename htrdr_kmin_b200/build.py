@@ -32,23 +32,42 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
-        return LIB
-    os.makedirs(LIBDIR, exist_ok=True)
-    tmp = LIB + ".tmp"
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared",
+def _compile(src: str, obj: str, verbose: bool) -> str:
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-c",
            "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
-           "-I", os.path.join(ROOT, "include"), "-o", tmp, *sources(), "-lpthread"]
+           "-I", os.path.join(ROOT, "include"), "-o", obj, src]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libhtrdr_gpu.so")
+        raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n{r.stdout}{r.stderr}")
+    return r.stderr if verbose else ""
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object (in parallel: the kernel variants
+    make each translation unit slow) and link the shared library."""
+    if not force and not _stale():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+    # the largest translation units first
+    order = sorted(range(len(srcs)), key=lambda i: -os.path.getsize(srcs[i]))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        futs = [ex.submit(_compile, srcs[i], objs[i], verbose) for i in order]
+        logs = [f.result() for f in futs]
     if verbose:
-        sys.stderr.write(r.stderr)
+        sys.stderr.write("".join(logs))
+    tmp = LIB + ".tmp"
+    r = subprocess.run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lpthread"],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed linking libhtrdr_gpu.so")
     os.replace(tmp, LIB)
     return LIB
 

@@ -29,7 +29,7 @@
 
 namespace hg {
 
-template <bool MESH>
+template <unsigned V>
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
 k_persistent(PTables T, int tables_in_smem)
 {
@@ -51,7 +51,7 @@ k_persistent(PTables T, int tables_in_smem)
   for(uint32_t it = 0;; ++it) {
     const unsigned tmask = __ballot_sync(0xffffffffu, p.state == ST_TRACE);
     if(tmask && (it % period) != 0) { /* not a regrouping step: tracing lanes only */
-      if(p.state == ST_TRACE) trace_step(p, T.scenes[p.si]);
+      if(p.state == ST_TRACE) trace_step<V>(p, T.scenes[p.si]);
       continue;
     }
     /* refill the private chunk of lanes that are idle with nothing left */
@@ -76,12 +76,12 @@ k_persistent(PTables T, int tables_in_smem)
       const DRequest& R = T.reqs[p.ri];
       const DScene& S = T.scenes[p.si];
       if(p.state != ST_TRACE && p.state != ST_DONE) {
-        path_event<MESH>(p, S, R);
+        path_event<V>(p, S, R);
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
         p.c_seg = p.c_node = p.c_tc = 0;
       }
       if(p.state == ST_TRACE) {
-        trace_step(p, S);
+        trace_step<V>(p, S);
       } else if(p.state == ST_DONE) {
         accumulate_b(p, R);
         real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
@@ -94,6 +94,13 @@ k_persistent(PTables T, int tables_in_smem)
   }
   seg += p.c_seg; node += p.c_node; tc += p.c_tc;
   flush_counts(T.cnt, seg, node, tc, real, fail);
+}
+
+using PersistentFn = void (*)(PTables, int);
+static PersistentFn
+persistent_fn(uint32_t v)
+{
+  HG_PICK_VARIANT(v, k_persistent)
 }
 
 bool
@@ -112,7 +119,7 @@ launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
   const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
   const int in_smem = tables <= 96 * 1024;
   const size_t smem = in_smem ? tables : 0;
-  auto kern = T.has_mesh ? k_persistent<true> : k_persistent<false>;
+  auto kern = persistent_fn(T.variant);
   if(smem > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
@@ -175,7 +182,7 @@ launch_workqueue_single(const DScene& S, const DRequest& R, void* tables, void* 
   T.items = &d->item;
   T.offsets = d->offsets;
   T.nscenes = 1;
-  T.has_mesh = S.g_ntris != 0;
+  T.variant = hv_make(S.g_ntris != 0, hv_kind(R.mode));
   T.nreqs = 1;
   T.nitems = 1;
   T.total = h.offsets[1];
@@ -190,7 +197,7 @@ persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device)
 {
   int nsm = 0, per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<true>, (int)block_size, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<HV_ALL>, (int)block_size, 0);
   if(blocks_per_sm) per_sm = std::min(per_sm, (int)blocks_per_sm);
   return (uint64_t)std::max(per_sm, 1) * (uint64_t)nsm * block_size;
 }
@@ -273,7 +280,7 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
   T.items = (const PItem*)P.d_items.ptr;
   T.offsets = (const uint64_t*)P.d_offsets.ptr;
   T.nscenes = (uint32_t)P.scenes.size();
-  T.has_mesh = std::any_of(P.scenes.begin(), P.scenes.end(), [](const DScene& d) { return d.g_ntris != 0; });
+  T.variant = tables_variant(P.scenes, P.reqs);
   T.nreqs = (uint32_t)n;
   T.nitems = (uint32_t)n;
   T.total = P.offsets[n];
@@ -433,7 +440,7 @@ extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best, double* best_ms)
 {
   if(!items || !n || !best) return HTRDR_GPU_RES_BAD_ARG;
-  static const uint32_t blocks[] = {128, 256};
+  static const uint32_t blocks[] = {96, 128, 256}; /* 96: 3 blocks of 3 warps fill 9 warps at 216 registers */
   static const uint32_t chunks[] = {1, 4};
   static const uint32_t periods[] = {1, 4, 16, 64};
   static const uint32_t tails[] = {25000, 100000};

@@ -29,6 +29,41 @@
 enum { HG_KA = 0, HG_KS = 1, HG_KEXT = 2 };
 enum { HG_XWAVE_SW = 0, HG_XWAVE_LW = 1, HG_IMAGE_CIE = 2, HG_FLUX_SW = 3, HG_FLUX_LW = 4 };
 
+/* Kernel variants: the parts of the path state machine one launch compiles.
+ * A launch whose requests are all shortwave (or all longwave) leaves out the
+ * other kind's states and trace filters, and a launch over plane-ground
+ * scenes leaves out the mesh queries: fewer registers and spills, and less
+ * code per warp.  A path of a kind its variant leaves out ends as a failed
+ * realisation (never a stuck one). */
+enum : uint32_t { HV_MESH = 1u, HV_SW = 2u, HV_LW = 4u, HV_ALL = 7u };
+
+/* Spectral kind of an output mode (HV_SW or HV_LW) */
+static inline uint32_t
+hv_kind(int mode)
+{
+  return (mode == HG_XWAVE_LW || mode == HG_FLUX_LW) ? HV_LW : HV_SW;
+}
+
+/* A variant from the launch's mesh flag and kinds (no kind: both) */
+static inline uint32_t
+hv_make(bool mesh, uint32_t kinds)
+{
+  kinds &= HV_SW | HV_LW;
+  return (mesh ? HV_MESH : 0u) | (kinds ? kinds : HV_SW | HV_LW);
+}
+
+/* Body of a host function returning kernel template K's instance for the
+ * variant v */
+#define HG_PICK_VARIANT(v, K)                                              \
+  switch(hv_make(((v) & HV_MESH) != 0, (v))) {                             \
+    case 2u: return K<2u>;                                                 \
+    case 3u: return K<3u>;                                                 \
+    case 4u: return K<4u>;                                                 \
+    case 5u: return K<5u>;                                                 \
+    case 6u: return K<6u>;                                                 \
+    default: return K<7u>;                                                 \
+  }
+
 struct DScene {
   /* gas column */
   uint32_t nlayers;

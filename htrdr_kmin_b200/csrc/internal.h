@@ -151,8 +151,18 @@ struct PTables {
   unsigned long long* next; /* queue head (zeroed before the launch) */
   void* cnt;                /* Counters (zeroed before the launch) */
   uint32_t chunk, regroup_period;
-  uint32_t has_mesh;        /* some scene has a ground mesh (selects the kernels' variant) */
+  uint32_t variant = HV_ALL; /* kernel variant (HV_* bits): the scenes' ground and the requests' kinds */
 };
+/* Kernel variant of a launch over these scenes and requests */
+inline uint32_t
+tables_variant(const std::vector<DScene>& scenes, const std::vector<DRequest>& reqs)
+{
+  bool mesh = false;
+  uint32_t kinds = 0;
+  for(const DScene& d : scenes) mesh = mesh || d.g_ntris != 0;
+  for(const DRequest& r : reqs) kinds |= hv_kind(r.mode);
+  return hv_make(mesh, kinds);
+}
 cudaError_t launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
                               int device, cudaStream_t st);
 bool valid_tuning(const htrdr_gpu_tuning& t);

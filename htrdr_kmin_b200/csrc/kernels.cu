@@ -9,14 +9,14 @@
 
 namespace hg {
 
-template <bool MESH>
+template <unsigned V>
 __device__ __forceinline__ void
 run_path(Path& p, const DScene& S, const DRequest& R)
 {
   for(;;) {
-    if(p.state == ST_TRACE) trace_step(p, S);
+    if(p.state == ST_TRACE) trace_step<V>(p, S);
     else if(p.state == ST_DONE) return;
-    else path_event<MESH>(p, S, R);
+    else path_event<V>(p, S, R);
   }
 }
 
@@ -59,7 +59,7 @@ flush_counters(Counters* cnt, unsigned long long seg, unsigned long long node,
   }
 }
 
-template <bool MESH>
+template <unsigned V>
 __global__ void __maxnreg__(HG_PLAIN_MAXNREG)
 k_plain(DScene S, DRequest R, DAccum* acc, DAccum* tacc, uint64_t pix_begin, uint32_t npix,
         double* weights, Counters* cnt)
@@ -73,7 +73,7 @@ k_plain(DScene S, DRequest R, DAccum* acc, DAccum* tacc, uint64_t pix_begin, uin
     p.pix = (uint32_t)(pix_begin + idx % npix);
     p.state = ST_GEN;
     p.flags = 0;
-    run_path<MESH>(p, S, R);
+    run_path<V>(p, S, R);
     if(weights) {
       weights[(idx % npix) * R.nreal_pp + p.ireal] =
         (p.flags & (PF_REJECTED | PF_FAILED)) ? __longlong_as_double(0x7ff8000000000000ll) : p.weight;
@@ -166,7 +166,7 @@ k_finalize(DRequest R, const DAccum* acc, const DAccum* tacc, char* out, size_t 
 /*******************************************************************************
  * Batched radiance (atmosphere_compute_radiance_sw/_lw with one stream per ray)
  ******************************************************************************/
-template <bool MESH>
+template <unsigned V>
 __global__ void __launch_bounds__(128)
 k_radiance(DScene S, int lw, size_t n, const double* pos, const double* dir, const double* wlen,
            const uint32_t* band, const uint32_t* iquad, int mask, uint32_t seed, double* out)
@@ -189,7 +189,7 @@ k_radiance(DScene S, int lw, size_t n, const double* pos, const double* dir, con
   p.flags = lw ? PF_LW : (((mask & 1) ? PF_DIRECT : 0u) | ((mask & 2) ? PF_DIFFUSE : 0u));
   p.c_seg = p.c_node = p.c_tc = 0;
   p.state = ST_RAD_BEGIN;
-  run_path<MESH>(p, S, R);
+  run_path<V>(p, S, R);
   out[i] = (p.flags & PF_FAILED) ? __longlong_as_double(0x7ff8000000000000ll) : p.weight;
 }
 
@@ -263,6 +263,26 @@ k_sample_wavelength(DRequest R, int channel, size_t n, const double* r0, const d
 static inline unsigned
 nblocks(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
 
+using PlainFn = void (*)(DScene, DRequest, DAccum*, DAccum*, uint64_t, uint32_t, double*, Counters*);
+static PlainFn
+plain_fn(uint32_t v)
+{
+  HG_PICK_VARIANT(v, k_plain)
+}
+
+using RadianceFn = void (*)(DScene, int, size_t, const double*, const double*, const double*,
+                            const uint32_t*, const uint32_t*, int, uint32_t, double*);
+static RadianceFn
+radiance_fn(uint32_t v)
+{
+  switch(v) {
+    case HV_SW: return k_radiance<HV_SW>;
+    case HV_SW | HV_MESH: return k_radiance<HV_SW | HV_MESH>;
+    case HV_LW: return k_radiance<HV_LW>;
+    default: return k_radiance<HV_LW | HV_MESH>;
+  }
+}
+
 cudaError_t
 launch_plain(const DScene& S, const DRequest& R, DAccum* acc, DAccum* tacc, uint64_t pix_begin,
              uint32_t npix, double* weights, void* counters, cudaStream_t st)
@@ -272,7 +292,7 @@ launch_plain(const DScene& S, const DRequest& R, DAccum* acc, DAccum* tacc, uint
   DRequest Ra = R;
   Ra.acc = acc;
   Ra.tacc = tacc;
-  auto kern = S.g_ntris ? k_plain<true> : k_plain<false>;
+  auto kern = plain_fn(hv_make(S.g_ntris != 0, hv_kind(R.mode)));
   kern<<<nblocks(total, 128), 128, 0, st>>>(S, Ra, acc, tacc, pix_begin, npix, weights,
                                             (Counters*)counters);
   note_launches(1);
@@ -298,7 +318,7 @@ launch_radiance(const DScene& S, int lw, size_t n, const double* pos, const doub
                 uint32_t seed, double* out, cudaStream_t st)
 {
   if(!n) return cudaSuccess;
-  auto kern = S.g_ntris ? k_radiance<true> : k_radiance<false>;
+  auto kern = radiance_fn(hv_make(S.g_ntris != 0, lw ? HV_LW : HV_SW));
   kern<<<nblocks(n, 128), 128, 0, st>>>(S, lw, n, pos, dir, wlen, band, iquad, mask, seed, out);
   return cudaGetLastError();
 }

@@ -147,6 +147,8 @@ struct htrdr_gpu_server {
   std::vector<uint32_t> w_scene_refs;          /* active requests per scene-table slot */
   std::vector<uint32_t> w_free_rslots;
   uint32_t w_nreqs = 0;                        /* request-table high-water mark */
+  uint32_t w_kinds = 0;                        /* spectral kinds admitted so far (HV_SW, HV_LW):
+                                                * the pool may hold paths of each */
   uint64_t w_nitems = 0, w_appended = 0;       /* queue: items and realisations appended */
   std::vector<uint64_t> w_offsets_host;        /* [w_nitems + 1] */
   bool w_pool_live = false;                    /* slots hold paths (not all free) */
@@ -215,7 +217,7 @@ htrdr_gpu_server::launch_round(Slot& s, const std::vector<SReq*>& act)
   T.items = (const PItem*)s.items.ptr;
   T.offsets = (const uint64_t*)s.offsets.ptr;
   T.nscenes = (uint32_t)scenes.size();
-  T.has_mesh = std::any_of(scenes.begin(), scenes.end(), [](const DScene& d) { return d.g_ntris != 0; });
+  T.variant = tables_variant(scenes, reqs);
   T.nreqs = (uint32_t)reqs.size();
   T.nitems = (uint32_t)items.size();
   T.total = offsets.back();
@@ -426,6 +428,7 @@ htrdr_gpu_server::wave_admit(SReq* r)
   r->sslot = ss;
   ++w_scene_refs[ss];
   w_nreqs = std::max(w_nreqs, rs + 1);
+  w_kinds |= hv_kind(r->dreq.mode);
   r->next = 0;
   return true;
 }
@@ -483,8 +486,9 @@ htrdr_gpu_server::wave_tables_now()
   T.items = (const PItem*)w_items.ptr;
   T.offsets = (const uint64_t*)w_offsets.ptr;
   T.nscenes = (uint32_t)w_scene_of.size();
-  T.has_mesh = std::any_of(w_scene_of.begin(), w_scene_of.end(),
-                           [](const htrdr_gpu_scene* sc) { return sc && sc->d.g_ntris != 0; });
+  T.variant = hv_make(std::any_of(w_scene_of.begin(), w_scene_of.end(),
+                                  [](const htrdr_gpu_scene* sc) { return sc && sc->d.g_ntris != 0; }),
+                      w_kinds);
   T.nreqs = w_nreqs;
   T.nitems = (uint32_t)w_nitems;
   T.total = w_appended;

@@ -351,12 +351,12 @@ ground_trace(const DScene& S, float3 o, float3 d, float r0, float r1, bool prev_
  * plane: distance in [0, r1) (< 0: none), the hit primitive, whether the hit
  * lies on an edge and the geometric normal.  `prev' says the ray leaves the
  * ground at (prev_prim, prev_edge). */
-template <bool MESH>
+template <unsigned V>
 __device__ __forceinline__ float
 ground_query(const DScene& S, float3 o, float3 d, float r1, bool prev, uint32_t prev_prim,
              bool prev_edge, uint32_t* prim, bool* edge, float3* ng)
 {
-  if(!MESH || !S.g_ntris) {
+  if(!(V & HV_MESH) || !S.g_ntris) {
     *prim = 0;
     *edge = false;
     *ng = make_float3(0.f, 0.f, 1.f);
@@ -381,12 +381,12 @@ struct SurfProps {
   int specular;
 };
 
-template <bool MESH>
+template <unsigned V>
 __device__ __forceinline__ SurfProps
 surface_props(const DScene& S, Rng& rng, float3 dir, uint32_t prim, float3 ng, double wlen_nm)
 {
   SurfProps s;
-  if(!MESH || !S.g_ntris) {
+  if(!(V & HV_MESH) || !S.g_ntris) {
     s.N = make_float3(0.f, 0.f, 1.f);
     s.refl = S.ground_refl;
     s.specular = S.ground_brdf == 1;
@@ -631,16 +631,20 @@ site_of(const DScene& S, const Trace& T, bool cloud, const uint32_t lo[3], const
 
 /* The hit filters (..._sw.c:73-217, ..._lw.c:64-135) on voxel [d0, d1].
  * Returns true when the traversal stops (real collision). */
+template <unsigned V>
 __device__ __forceinline__ bool
 voxel_filter(Path& p, const DScene& S, float d0, float d1, float kmin, float kmax, bool cloud,
              const uint32_t lo[3], const uint32_t hi[3])
 {
   Trace& T = p.tr;
+  /* the kinds the variant can meet (a LW-only variant meets TK_LW alone) */
+  const bool trans = (V & HV_SW) && T.kind == TK_TRANS;
+  const bool scat = (V & HV_SW) && (!(V & HV_LW) || T.kind == TK_SCATTER);
   /* the traversed distance is carried in FP64 inside the voxel so that tiny
    * free paths still advance it far from the origin */
   double tc = (double)d0;
   const double e = (double)d1;
-  if(T.kind == TK_TRANS) {
+  if(trans) {
     T.Tmin += (e - tc) * (double)kmin;
     if(T.Tmin >= HG_TMIN_ZERO) return true; /* exp(-Tmin) is already 0.0 */
     const double kdif = (double)kmax - (double)kmin;
@@ -669,7 +673,7 @@ voxel_filter(Path& p, const DScene& S, float d0, float d1, float kmin, float kma
       int cell, layer;
       site_of(S, T, cloud, lo, hi, madd3(T.o, T.d, T.tcur), cell, layer);
       ++p.c_tc;
-      if(T.kind == TK_SCATTER) {
+      if(scat) {
         const float ks = site_k(S, cell, layer, p.band, p.q, HG_KS, 3);
         if(p.rng.uf() < ks / kmax) { T.site_cell = cell; T.site_layer = layer; return true; }
       } else {
@@ -715,16 +719,19 @@ gas_tau_at(const DScene& S, const double* cum, uint32_t q, int prop, double z)
  * free path the inversion of the cumulative depth at Ts.  The same random
  * numbers are consumed as in the layer-by-layer traversal.  Returns true when
  * the trace stops (real collision). */
+template <unsigned V>
 __device__ __forceinline__ bool
 gas_region(Path& p, const DScene& S, float re)
 {
   Trace& T = p.tr;
+  const bool trans = (V & HV_SW) && T.kind == TK_TRANS;
+  const bool scat = (V & HV_SW) && (!(V & HV_LW) || T.kind == TK_SCATTER);
   const double dz = (double)T.d.z, adz = fabs(dz);
   const double* cum = S.gas_cum + ((size_t)p.q * 3 + T.prop) * (S.nlayers + 1);
   double ta = (double)T.t;
   double tau_a = gas_tau_at(S, cum, p.q, T.prop, (double)T.o.z + dz * ta);
   const double tau_b = gas_tau_at(S, cum, p.q, T.prop, (double)T.o.z + dz * (double)re);
-  if(T.kind == TK_TRANS) {
+  if(trans) {
     T.Tmin += fabs(tau_b - tau_a) / adz;
     return T.Tmin >= HG_TMIN_ZERO; /* exp(-Tmin) is already 0.0 */
   }
@@ -755,7 +762,7 @@ gas_region(Path& p, const DScene& S, float re)
     t = fmin(fmax(t, ta), (double)re);
     T.tcur = (float)t;
     ++p.c_tc;
-    if(T.kind == TK_SCATTER) {
+    if(scat) {
       /* k_s max of a gas voxel is k_s itself: the test always accepts */
       if(p.rng.uf() < 1.0f) { T.site_cell = -1; T.site_layer = l; return true; }
     } else {
@@ -774,6 +781,7 @@ gas_region(Path& p, const DScene& S, float re)
 }
 
 /* One voxel of the current trace */
+template <unsigned V>
 __device__ __forceinline__ void
 trace_step(Path& p, const DScene& S)
 {
@@ -786,7 +794,7 @@ trace_step(Path& p, const DScene& S)
   region_bounds(T, T.region, rs, re, cloud);
   ++p.c_seg;
   if(!cloud && T.d.z != 0.f) { /* the whole gas region at once */
-    if(gas_region(p, S, re)) { trace_finish(p, true); return; }
+    if(gas_region<V>(p, S, re)) { trace_finish(p, true); return; }
     ++T.region;
     region_enter(T, S);
     return;
@@ -800,7 +808,7 @@ trace_step(Path& p, const DScene& S)
     if(t1 > T.t) {
       const float k = gas_k(S, p.q, T.prop, l);
       const uint32_t z3[3] = {0, 0, 0};
-      if(voxel_filter(p, S, T.t, t1, k, k, false, z3, z3)) { trace_finish(p, true); return; }
+      if(voxel_filter<V>(p, S, T.t, t1, k, k, false, z3, z3)) { trace_finish(p, true); return; }
     }
     if(tn >= re) { ++T.region; region_enter(T, S); return; }
     T.t = t1;
@@ -859,7 +867,7 @@ trace_step(Path& p, const DScene& S)
   }
   const float t1 = fmaxf(fminf(texit, re), T.t);
   if(t1 > T.t) {
-    if(voxel_filter(p, S, T.t, t1, __uint_as_float(v.x), __uint_as_float(v.y), true, lo, hi)) {
+    if(voxel_filter<V>(p, S, T.t, t1, __uint_as_float(v.x), __uint_as_float(v.y), true, lo, hi)) {
       trace_finish(p, true);
       return;
     }
@@ -1106,7 +1114,7 @@ struct ScatOut {
  * the next-event estimate with its phase/BRDF value
  * (htrdr_atmosphere_compute_radiance_sw.c:400-490).
  * Out of line: it runs once per scattering and holds the FP64 sun sampling. */
-template <bool MESH>
+template <unsigned V>
 __device__ __noinline__ ScatOut
 sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float refl,
            int site_cell, int site_layer, uint32_t band, uint32_t q, uint32_t gprim, float3 gN,
@@ -1121,7 +1129,7 @@ sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float 
   o.refl = refl;
   o.sdir = mk3(0.f, 0.f, 0.f);
   if(surface) {
-    const SurfProps sp = surface_props<MESH>(S, rng, dir, gprim, gN, wlen_nm);
+    const SurfProps sp = surface_props<V>(S, rng, dir, gprim, gN, wlen_nm);
     N = sp.N;
     brdf_specular = sp.specular;
     if(dot3(N, wo) < 0.f) N = neg3(N);
@@ -1164,10 +1172,19 @@ sw_scatter(const DScene& S, Rng rng, float3 dir, float g, uint32_t flags, float 
   return o;
 }
 
+/* A path of a kind the kernel variant leaves out: a failed realisation */
+__device__ __forceinline__ void
+path_variant_miss(Path& p)
+{
+  p.flags |= PF_FAILED;
+  p.state = ST_RAD_END;
+}
+
 /* Advance the state machine until the path needs a voxel step (ST_TRACE),
- * is done (ST_DONE) or idle.  MESH = false: the scenes of the launch have
- * the plane ground only (the mesh queries are compiled out). */
-template <bool MESH>
+ * is done (ST_DONE) or idle.  V: the kernel variant (HV_* bits); the states
+ * of a spectral kind it leaves out and, without HV_MESH, the mesh queries
+ * are compiled out. */
+template <unsigned V>
 __device__ __forceinline__ void
 path_event(Path& p, const DScene& S, const DRequest& R)
 {
@@ -1181,13 +1198,19 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         p.w = 0.0;
         p.ksi = 1.f;
         p.bounces = 0;
-        if(p.flags & PF_LW) { p.state = ST_LW_WALK; break; }
+        if(p.flags & PF_LW) {
+          if(V & HV_LW) p.state = ST_LW_WALK;
+          else path_variant_miss(p);
+          break;
+        }
+        if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; }
+        else {
         p.L_sun = planck_mono(p.wlen_d * 1e-9, S.sun_T);
         if((p.flags & PF_DIRECT) && ((p.flags & PF_IN_CONE) || in_solar_cone(S, p.dir))) {
           uint32_t hp;
           bool he;
           float3 hn;
-          if(ground_query<MESH>(S, p.pos, p.dir, FLT_MAX, false, 0u, false, &hp, &he, &hn) < 0.f) {
+          if(ground_query<V>(S, p.pos, p.dir, FLT_MAX, false, 0u, false, &hp, &he, &hn) < 0.f) {
             p.flags |= PF_TRACED;
             trace_begin(p, S, TK_TRANS, HG_KEXT, p.pos, p.dir, 0.f, FLT_MAX, ST_SW_DIRECT_END);
             return;
@@ -1195,21 +1218,25 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         }
         p.state = ST_SW_DIRECT_END;
         break;
+        }
       }
 
       case ST_SW_DIRECT_END:
-        if(p.flags & PF_TRACED) {
-          const double Tr = p.tr.hit ? 0.0 : (p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
-          p.w = p.L_sun * Tr;
+        if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; }
+        else {
+          if(p.flags & PF_TRACED) {
+            const double Tr = p.tr.hit ? 0.0 : (p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
+            p.w = p.L_sun * Tr;
+          }
+          p.state = (p.flags & PF_DIFFUSE) ? ST_SW_WALK : ST_RAD_END;
         }
-        p.state = (p.flags & PF_DIFFUSE) ? ST_SW_WALK : ST_RAD_END;
         break;
 
-      case ST_SW_WALK: {
+      case ST_SW_WALK: if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; } else {
         if(++p.bounces > HG_MAX_BOUNCES) { p.flags |= PF_FAILED; p.state = ST_RAD_END; break; }
         {
           bool e;
-          p.gdist = ground_query<MESH>(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
+          p.gdist = ground_query<V>(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
                                  p.prev_prim, p.prev_edge != 0, &p.gprim, &e, &p.gN);
           p.gedge = e;
         }
@@ -1219,7 +1246,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         return;
       }
 
-      case ST_SW_SCAT_END: {
+      case ST_SW_SCAT_END: if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; } else {
         const bool svx = p.tr.hit != 0;
         if(p.gdist < 0.f && !svx) { p.state = ST_RAD_END; break; }
         const bool surface = !svx;
@@ -1238,10 +1265,10 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         return;
       }
 
-      case ST_SW_ABS_END: {
+      case ST_SW_ABS_END: if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; } else {
         p.tr_abs = p.tr.hit ? 0.f : (float)(p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
         if(p.tr_abs <= 0.f) { p.state = ST_RAD_END; break; }
-        const ScatOut so = sw_scatter<MESH>(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
+        const ScatOut so = sw_scatter<V>(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
                                       p.site_layer, p.band, p.q, p.gprim, p.gN, p.wlen_d);
         p.rng = so.rng;
         p.flags = so.flags;
@@ -1254,7 +1281,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         bool he;
         float3 hn;
         if(p.R > 0.f
-        && ground_query<MESH>(S, p.pnext, p.sdir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0, p.prev_prim,
+        && ground_query<V>(S, p.pnext, p.sdir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0, p.prev_prim,
                         p.prev_edge != 0, &hp, &he, &hn) < 0.f) {
           p.flags |= PF_TRACED;
           trace_begin(p, S, TK_TRANS, HG_KEXT, p.pnext, p.sdir, 0.f, FLT_MAX, ST_SW_NEE_END);
@@ -1265,7 +1292,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         break;
       }
 
-      case ST_SW_NEE_END: {
+      case ST_SW_NEE_END: if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; } else {
         double Tr = 0.0;
         if(p.flags & PF_TRACED) Tr = p.tr.hit ? 0.0 : (p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
         p.flags &= ~PF_TRACED;
@@ -1278,11 +1305,11 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         break;
       }
 
-      case ST_LW_WALK: {
+      case ST_LW_WALK: if constexpr(!(V & HV_LW)) { path_variant_miss(p); break; } else {
         if(++p.bounces > HG_MAX_BOUNCES) { p.flags |= PF_FAILED; p.state = ST_RAD_END; break; }
         {
           bool e;
-          p.gdist = ground_query<MESH>(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
+          p.gdist = ground_query<V>(S, p.pos, p.dir, FLT_MAX, (p.flags & PF_PREV_GROUND) != 0,
                                  p.prev_prim, p.prev_edge != 0, &p.gprim, &e, &p.gN);
           p.gedge = e;
         }
@@ -1292,7 +1319,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
         return;
       }
 
-      case ST_LW_END: {
+      case ST_LW_END: if constexpr(!(V & HV_LW)) { path_variant_miss(p); break; } else {
         const bool svx = p.tr.hit != 0;
         const double wlen_m = p.wlen_d * 1e-9;
         if(p.gdist < 0.f && !svx) { p.w = 0.0; p.state = ST_RAD_END; break; }
@@ -1309,7 +1336,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
           p.dnext = around(p.dir, hg_mu(p.g, u1), u2);
           p.flags &= ~PF_PREV_GROUND;
         } else {
-          const SurfProps sp = surface_props<MESH>(S, p.rng, p.dir, p.gprim, p.gN, p.wlen_d);
+          const SurfProps sp = surface_props<V>(S, p.rng, p.dir, p.gprim, p.gN, p.wlen_d);
           float3 N = sp.N;
           const float3 wo = neg3(p.dir);
           if(dot3(N, wo) < 0.f) N = neg3(N);
@@ -1336,7 +1363,7 @@ path_event(Path& p, const DScene& S, const DRequest& R)
       }
 
       case ST_RAD_END:
-        if(R.mode == HG_FLUX_SW) {
+        if((V & HV_SW) && R.mode == HG_FLUX_SW) {
           if(!(p.flags & PF_STAGE2)) {
             p.wdirect = p.w;
             p.flags = (p.flags & ~(PF_DIRECT | PF_IN_CONE)) | PF_STAGE2 | PF_DIFFUSE;

@@ -93,7 +93,7 @@ struct WTables {
 
 /* Iteration parity b: the event stage reads list b and writes list b^1; the
  * trace stage then walks list b^1. */
-template <bool MESH>
+template <unsigned V>
 __global__ void __launch_bounds__(128)
 k_wave_event(WTables W, uint32_t b, int tables_in_smem)
 {
@@ -146,7 +146,7 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
       if(!__any_sync(0xffffffffu, busy)) break;
       if(busy) {
         if(p.state != ST_DONE) {
-          path_event<MESH>(p, T.scenes[p.si], T.reqs[p.ri]);
+          path_event<V>(p, T.scenes[p.si], T.reqs[p.ri]);
           seg += p.c_seg; node += p.c_node; tc += p.c_tc;
           p.c_seg = p.c_node = p.c_tc = 0;
         }
@@ -226,7 +226,7 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
     }
     if(!__any_sync(0xffffffffu, have)) break;
     if(have) {
-      trace_step(p, T.scenes[p.si]);
+      trace_step<HV_ALL>(p, T.scenes[p.si]);
       if(p.state != ST_TRACE || --left == 0) {
         p.t0 = gtimer() - p.t0;
         store_trace(p, W.paths + (size_t)s * kPathV4);
@@ -302,7 +302,7 @@ k_wave_clamp(WTables W)
  * live list 0 from their slots, then take any realisations left in the work
  * queue; events and traces run in the same thread, events regrouped every
  * `regroup_period' voxel steps as in the persistent engine. */
-template <bool MESH>
+template <unsigned V>
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
 k_wave_finish(WTables W, int tables_in_smem)
 {
@@ -324,7 +324,7 @@ k_wave_finish(WTables W, int tables_in_smem)
   for(uint32_t it = 0;; ++it) {
     const unsigned tmask = __ballot_sync(0xffffffffu, p.state == ST_TRACE);
     if(tmask && (it % period) != 0) {
-      if(p.state == ST_TRACE) trace_step(p, T.scenes[p.si]);
+      if(p.state == ST_TRACE) trace_step<V>(p, T.scenes[p.si]);
       continue;
     }
     /* idle lanes: a saved path of the live list first, then the queue */
@@ -365,12 +365,12 @@ k_wave_finish(WTables W, int tables_in_smem)
       const DRequest& R = T.reqs[p.ri];
       const DScene& S = T.scenes[p.si];
       if(p.state != ST_TRACE && p.state != ST_DONE) {
-        path_event<MESH>(p, S, R);
+        path_event<V>(p, S, R);
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
         p.c_seg = p.c_node = p.c_tc = 0;
       }
       if(p.state == ST_TRACE) {
-        trace_step(p, S);
+        trace_step<V>(p, S);
       } else if(p.state == ST_DONE) {
         accumulate_b(p, R);
         real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
@@ -431,6 +431,19 @@ wave_reserve(WaveBufs& B, uint32_t P)
 
 namespace {
 
+using WaveEventFn = void (*)(WTables, uint32_t, int);
+using WaveFinishFn = void (*)(WTables, int);
+WaveEventFn
+wave_event_fn(uint32_t v)
+{
+  HG_PICK_VARIANT(v, k_wave_event)
+}
+WaveFinishFn
+wave_finish_fn(uint32_t v)
+{
+  HG_PICK_VARIANT(v, k_wave_finish)
+}
+
 /* Launch shapes of a run over the tables T */
 struct WaveLaunch {
   size_t smem = 0;
@@ -450,8 +463,8 @@ wave_params(const PTables& T, const htrdr_gpu_tuning& tun, int device, WaveLaunc
   const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
   L.in_smem = tables <= 96 * 1024;
   L.smem = L.in_smem ? tables : 0;
-  L.ev = T.has_mesh ? k_wave_event<true> : k_wave_event<false>;
-  L.fi = T.has_mesh ? k_wave_finish<true> : k_wave_finish<false>;
+  L.ev = wave_event_fn(T.variant);
+  L.fi = wave_finish_fn(T.variant);
   cudaError_t e;
   if(L.smem > 48 * 1024) {
     if((e = cudaFuncSetAttribute(L.ev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
