@@ -31,7 +31,7 @@ KA, KS, KEXT = 0, 1, 2
 DIRECT, DIFFUSE, ALL = 1, 2, 3
 
 EXPORTED = [
-    "htrdr_gpu_scene_create", "htrdr_gpu_scene_release", "htrdr_gpu_scene_device_bytes",
+    "htrdr_gpu_scene_create", "htrdr_gpu_scene_create_cached", "htrdr_gpu_scene_release", "htrdr_gpu_scene_device_bytes",
     "htrdr_gpu_scene_get_tree", "htrdr_gpu_scene_tree_depth", "htrdr_gpu_draw_map",
     "htrdr_gpu_draw_map_device", "htrdr_gpu_radiance_sw", "htrdr_gpu_radiance_lw",
     "htrdr_gpu_realisation_weights", "htrdr_gpu_find_band", "htrdr_gpu_sample_quad",
@@ -174,6 +174,8 @@ def lib() -> C.CDLL:
     L = C.CDLL(LIB_PATH)
     vp, sz, u32, i32, dp, up = C.c_void_p, C.c_size_t, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p
     L.htrdr_gpu_scene_create.argtypes = [C.c_int, C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]
+    L.htrdr_gpu_scene_create_cached.argtypes = [C.c_int, C.POINTER(SceneDesc), C.c_char_p,
+                                                C.POINTER(C.c_void_p)]
     L.htrdr_gpu_scene_release.argtypes = [vp]
     L.htrdr_gpu_scene_release.restype = None
     L.htrdr_gpu_scene_device_bytes.argtypes = [vp]
@@ -264,7 +266,9 @@ class GpuScene:
     """A scene resident in HBM with its majorant octrees (htsky_create)."""
 
     def __init__(self, scene: S.Scene, props_mask: int = 0b111, device: int = 0,
-                 octree_on_host: bool = False):
+                 octree_on_host: bool = False, cache_path: Optional[str] = None):
+        """cache_path: the octree cache of option -O (loaded when it holds
+        this medium's octrees, written when it does not exist)."""
         scene.validate()
         self.scene = scene
         keep: List[np.ndarray] = []
@@ -310,7 +314,11 @@ class GpuScene:
         if scene.ground_mesh is not None:
             scene.ground_mesh.fill_desc(d, keep)
         h = C.c_void_p()
-        _check(lib().htrdr_gpu_scene_create(device, C.byref(d), C.byref(h)), "htrdr_gpu_scene_create")
+        if cache_path is not None:
+            _check(lib().htrdr_gpu_scene_create_cached(device, C.byref(d), os.fsencode(cache_path),
+                                                       C.byref(h)), "htrdr_gpu_scene_create_cached")
+        else:
+            _check(lib().htrdr_gpu_scene_create(device, C.byref(d), C.byref(h)), "htrdr_gpu_scene_create")
         self.handle = h
 
     def close(self):

@@ -13,7 +13,10 @@
 #include <atomic>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <memory>
+#include <string>
 #include <thread>
 
 namespace hg {
@@ -459,8 +462,173 @@ htrdr_gpu_device_count(void)
 extern "C" HTRDR_GPU_API const char*
 htrdr_gpu_version(void) { return "htrdr_gpu 0.1 (sm_100a)"; }
 
+namespace {
+
+/* ---- majorant-octree cache (option -O) ----
+ * File: a 64-byte header {magic "HGOCTREE", format 1, medium signature,
+ * octree depth, quadrature points, property mask, node count}, then the
+ * first node and node count of each (quad point, property) tree as u64
+ * [nq][3] each, then the nodes (16 bytes each, device layout). */
+constexpr char kCacheMagic[8] = {'H', 'G', 'O', 'C', 'T', 'R', 'E', 'E'};
+constexpr uint64_t kCacheFormat = 1;
+
+struct CacheHeader {
+  char magic[8];
+  uint64_t format;
+  uint64_t signature;
+  uint32_t depth, nq, props_mask, pad;
+  uint64_t nodes;
+  uint64_t reserved[2];
+};
+static_assert(sizeof(CacheHeader) == 64, "cache header layout");
+
+/* 64-bit signature of a byte range, 8 bytes per step (FNV-1a on words
+ * with a final avalanche); enough to tell two media apart */
+struct Signature {
+  uint64_t h = 0xcbf29ce484222325ull;
+  void add(const void* data, size_t bytes)
+  {
+    const unsigned char* c = (const unsigned char*)data;
+    size_t i = 0;
+    for(; i + 8 <= bytes; i += 8) {
+      uint64_t w;
+      std::memcpy(&w, c + i, 8);
+      h = (h ^ w) * 0x100000001b3ull;
+    }
+    uint64_t w = 0;
+    std::memcpy(&w, c + i, bytes - i);
+    h = (h ^ w ^ (uint64_t)bytes) * 0x100000001b3ull;
+  }
+  template <typename T> void add_val(T v) { add(&v, sizeof(v)); }
+  uint64_t done() const
+  {
+    uint64_t x = h;
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull;
+    return x ^ (x >> 33);
+  }
+};
+
+/* The inputs the octrees depend on, but -T and -V (which the cache
+ * overrides) and the options of the traversal (-r) */
+uint64_t
+medium_signature(const htrdr_gpu_scene_desc* d, uint32_t nq)
+{
+  Signature g;
+  const uint32_t nl = d->nlayers, nb = d->nbands;
+  g.add_val(nl);
+  g.add(d->layer_z, (nl + 1) * sizeof(double));
+  g.add(d->layer_T, nl * sizeof(float));
+  g.add_val(nb);
+  g.add(d->band_lo, nb * sizeof(double));
+  g.add(d->band_hi, nb * sizeof(double));
+  g.add(d->nquads, nb * sizeof(uint32_t));
+  g.add(d->quad_w, nq * sizeof(double));
+  g.add(d->gas_ka, (size_t)nq * nl * sizeof(float));
+  g.add(d->gas_ks, (size_t)nq * nl * sizeof(float));
+  g.add(d->cloud_def, sizeof(d->cloud_def));
+  g.add(d->cloud_lower, sizeof(d->cloud_lower));
+  g.add(d->cloud_cell, sizeof(d->cloud_cell));
+  g.add(d->cloud_lwc, (size_t)d->cloud_def[0] * d->cloud_def[1] * d->cloud_def[2] * sizeof(float));
+  if(d->cloud_sigma_ext) g.add(d->cloud_sigma_ext, nb * sizeof(float));
+  if(d->cloud_ssa) g.add(d->cloud_ssa, nb * sizeof(float));
+  if(d->cloud_g) g.add(d->cloud_g, nb * sizeof(float));
+  g.add_val(d->props_mask & 7u);
+  return g.done();
+}
+
+/* Reads the cache into host tables; false with the error set when the file
+ * is unreadable or was written from another medium */
+bool
+cache_read(const char* path, uint64_t signature, uint32_t depth, uint32_t nq, uint32_t props_mask,
+           std::vector<uint64_t>& base, std::vector<uint64_t>& count, std::vector<uint32_t>& nodes)
+{
+  std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path, "rb"), &std::fclose);
+  CacheHeader h;
+  if(!f || std::fread(&h, sizeof(h), 1, f.get()) != 1 || std::memcmp(h.magic, kCacheMagic, 8)
+  || h.format != kCacheFormat) {
+    set_error(std::string("octree cache `") + path + "': not an octree cache of this library");
+    return false;
+  }
+  if(h.signature != signature || h.depth != depth || h.nq != nq || h.props_mask != (props_mask & 7u)) {
+    set_error(std::string("octree cache `") + path + "' was built from other inputs");
+    return false;
+  }
+  base.resize((size_t)nq * 3);
+  count.resize((size_t)nq * 3);
+  nodes.resize((size_t)h.nodes * 4);
+  if(std::fread(base.data(), 8, base.size(), f.get()) != base.size()
+  || std::fread(count.data(), 8, count.size(), f.get()) != count.size()
+  || std::fread(nodes.data(), 16, h.nodes, f.get()) != h.nodes) {
+    set_error(std::string("octree cache `") + path + "': truncated");
+    return false;
+  }
+  for(size_t i = 0; i < base.size(); ++i)
+    if(count[i] && (base[i] > h.nodes || count[i] > h.nodes - base[i])) {
+      set_error(std::string("octree cache `") + path + "': tree out of range");
+      return false;
+    }
+  return true;
+}
+
+/* Writes the cache (to a temporary file renamed into place) */
+bool
+cache_write(const char* path, uint64_t signature, uint32_t depth, uint32_t nq, uint32_t props_mask,
+            const std::vector<uint64_t>& base, const std::vector<uint64_t>& count,
+            const uint32_t* nodes, uint64_t nnodes)
+{
+  const std::string tmp = std::string(path) + ".tmp";
+  CacheHeader h{};
+  std::memcpy(h.magic, kCacheMagic, 8);
+  h.format = kCacheFormat;
+  h.signature = signature;
+  h.depth = depth;
+  h.nq = nq;
+  h.props_mask = props_mask & 7u;
+  h.nodes = nnodes;
+  bool ok;
+  {
+    std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(tmp.c_str(), "wb"), &std::fclose);
+    ok = f && std::fwrite(&h, sizeof(h), 1, f.get()) == 1
+      && std::fwrite(base.data(), 8, base.size(), f.get()) == base.size()
+      && std::fwrite(count.data(), 8, count.size(), f.get()) == count.size()
+      && std::fwrite(nodes, 16, nnodes, f.get()) == nnodes;
+    if(f && std::fflush(f.get()) != 0) ok = false;
+  }
+  if(ok && std::rename(tmp.c_str(), path) != 0) ok = false;
+  if(!ok) {
+    std::remove(tmp.c_str());
+    set_error(std::string("octree cache `") + path + "': cannot write");
+  }
+  return ok;
+}
+
+htrdr_gpu_res_T scene_create(int device, const htrdr_gpu_scene_desc* desc, const char* cache_path,
+                             htrdr_gpu_scene** out);
+
+}  // namespace
+
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_scene** out)
+{
+  return scene_create(device, desc, nullptr, out);
+}
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_scene_create_cached(int device, const htrdr_gpu_scene_desc* desc, const char* cache_path,
+                              htrdr_gpu_scene** out)
+{
+  if(!cache_path || !*cache_path) {
+    set_error("no cache path");
+    return HTRDR_GPU_RES_BAD_ARG;
+  }
+  return scene_create(device, desc, cache_path, out);
+}
+
+namespace {
+
+htrdr_gpu_res_T
+scene_create(int device, const htrdr_gpu_scene_desc* desc, const char* cache_path, htrdr_gpu_scene** out)
 {
   if(!desc || !out || !desc->nlayers || !desc->nbands || !desc->layer_z || !desc->layer_T
   || !desc->band_lo || !desc->band_hi || !desc->nquads || !desc->quad_w || !desc->gas_ka
@@ -615,7 +783,23 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
     for(uint32_t q = 0; q < nq; ++q)
       for(int p = 0; p < 3; ++p)
         if(desc->props_mask & (1u << p)) tasks.emplace_back(q, p);
-    if(desc->octree_on_host) { /* host build, in parallel over the trees */
+    const uint64_t signature = cache_path ? medium_signature(desc, nq) : 0;
+    bool cached = false;
+    if(cache_path) { /* an existing cache replaces the build (-O) */
+      std::unique_ptr<FILE, int (*)(FILE*)> probe(std::fopen(cache_path, "rb"), &std::fclose);
+      if(probe) {
+        probe.reset();
+        std::vector<uint32_t> nodes;
+        if(!cache_read(cache_path, signature, D, nq, desc->props_mask, scn->tree_base, scn->tree_count, nodes))
+          return HTRDR_GPU_RES_BAD_ARG;
+        if(!(S.nodes = (const uint4*)upload(nodes.data(), std::max<size_t>(nodes.size(), 4) * 4)))
+          return HTRDR_GPU_RES_MEM_ERR;
+        cached = true;
+      }
+    }
+    if(cached) {
+      /* loaded */
+    } else if(desc->octree_on_host) { /* host build, in parallel over the trees */
       std::vector<std::vector<uint32_t>> trees(tasks.size());
       std::atomic<size_t> next(0);
       const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -647,6 +831,10 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
         std::memcpy(&pool_nodes[scn->tree_base[idx] * 4], trees[i].data(), trees[i].size() * 4);
       }
       if(!(S.nodes = (const uint4*)upload(pool_nodes.data(), total * 4))) return HTRDR_GPU_RES_MEM_ERR;
+      if(cache_path
+      && !cache_write(cache_path, signature, D, nq, desc->props_mask, scn->tree_base, scn->tree_count,
+                      pool_nodes.data(), total / 4))
+        return HTRDR_GPU_RES_IO_ERR;
     } else { /* GPU build (octree_gpu.cu), same node arrays */
       DevBuf d_ka, d_ks;
       auto pool = std::make_unique<DevBuf>();
@@ -663,6 +851,16 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
       }
       S.nodes = (const uint4*)pool->ptr;
       scn->bytes += pool->bytes;
+      if(cache_path) {
+        uint64_t total = 0;
+        for(size_t i = 0; i < base.size(); ++i) total = std::max(total, base[i] + count[i]);
+        std::vector<uint32_t> host((size_t)total * 4);
+        if(total && !cuda_ok(cudaMemcpy(host.data(), pool->ptr, total * 16, cudaMemcpyDeviceToHost), "D2H"))
+          return HTRDR_GPU_RES_UNKNOWN_ERR;
+        if(!cache_write(cache_path, signature, D, nq, desc->props_mask, scn->tree_base, scn->tree_count,
+                        host.data(), total))
+          return HTRDR_GPU_RES_IO_ERR;
+      }
       scn->bufs.push_back(std::move(pool));
     }
     if(!(S.tree_base = (const uint64_t*)upload(scn->tree_base.data(), scn->tree_base.size() * 8)))
@@ -698,6 +896,8 @@ htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_s
   *out = scn.release();
   return HTRDR_GPU_RES_OK;
 }
+
+}  // namespace
 
 extern "C" HTRDR_GPU_API void
 htrdr_gpu_scene_release(htrdr_gpu_scene* scn)

@@ -150,6 +150,17 @@ struct htrdr_gpu_server;
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_create(int device, const struct htrdr_gpu_scene_desc* desc,
                        struct htrdr_gpu_scene** scene);
+/* The same with the majorant-octree cache of option -O (htsky's
+ * cache_filename, src/atmosphere/htrdr_atmosphere.c:369): when `cache_path'
+ * exists and was written from the same medium (layers, gas and cloud
+ * coefficients, optics, spectral grid, octree properties) its octrees are
+ * loaded instead of built, and optical_thickness and grid_max_definition
+ * (-T, -V) are ignored; when it holds octrees of another medium the call
+ * fails with RES_BAD_ARG; when it does not exist the octrees are built and
+ * written to it.  The file stores 16-byte nodes in the device layout. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_scene_create_cached(int device, const struct htrdr_gpu_scene_desc* desc,
+                              const char* cache_path, struct htrdr_gpu_scene** scene);
 HTRDR_GPU_API void htrdr_gpu_scene_release(struct htrdr_gpu_scene* scene);
 /* Device bytes held by the scene (medium + octrees) */
 HTRDR_GPU_API size_t htrdr_gpu_scene_device_bytes(const struct htrdr_gpu_scene* scene);
