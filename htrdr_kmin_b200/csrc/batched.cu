@@ -29,16 +29,13 @@
 
 namespace hg {
 
+/* The persistent loop over one lane's path `p' (in registers or in shared
+ * memory: see k_persistent) */
 template <unsigned V>
-__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
-k_persistent(PTables T, int tables_in_smem)
+__device__ __forceinline__ void
+persistent_loop(PTables& T, Path& p)
 {
-  /* the scene and request views are read on every step: keep them in shared
-   * memory when they fit (one copy per block) */
-  extern __shared__ __align__(16) unsigned char smem[];
-  if(tables_in_smem) tables_to_smem(T, smem);
   const unsigned lane = threadIdx.x & 31u;
-  Path p;
   p.state = ST_IDLE;
   p.flags = 0;
   p.c_seg = p.c_node = p.c_tc = 0;
@@ -96,6 +93,25 @@ k_persistent(PTables T, int tables_in_smem)
   flush_counts(T.cnt, seg, node, tc, real, fail);
 }
 
+template <unsigned V>
+__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
+k_persistent(PTables T, int tables_in_smem)
+{
+  /* the scene and request views are read on every step: keep them in shared
+   * memory when they fit (one copy per block), after the block's paths when
+   * these live there too */
+  extern __shared__ __align__(16) unsigned char smem[];
+  if constexpr(persistent_smem_paths(V)) {
+    PathSlot* slots = (PathSlot*)smem;
+    if(tables_in_smem) tables_to_smem(T, smem + path_slots_bytes(blockDim.x));
+    persistent_loop<V>(T, slots[threadIdx.x].p);
+  } else {
+    if(tables_in_smem) tables_to_smem(T, smem);
+    Path p;
+    persistent_loop<V>(T, p);
+  }
+}
+
 using PersistentFn = void (*)(PTables, int);
 static PersistentFn
 persistent_fn(uint32_t v)
@@ -118,8 +134,10 @@ launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
   if(!T.total) return cudaSuccess;
   const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
   const int in_smem = tables <= 96 * 1024;
-  const size_t smem = in_smem ? tables : 0;
-  auto kern = persistent_fn(T.variant);
+  const uint32_t v = hv_make((T.variant & HV_MESH) != 0, T.variant);
+  const size_t smem = (in_smem ? tables : 0) + (persistent_smem_paths(v) ? path_slots_bytes(block_size) : 0);
+  auto kern = persistent_fn(v);
+  if(smem > 227 * 1024) return cudaErrorInvalidConfiguration; /* block too large for its paths */
   if(smem > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);

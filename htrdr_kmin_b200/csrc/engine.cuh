@@ -102,6 +102,36 @@ flush_counts(void* cnt, unsigned long long seg, unsigned long long node, unsigne
 
 /* Copy the scene and request tables of a launch into shared memory (one
  * copy per block) and point T at them */
+/* A path held in shared memory.  8 bytes of padding give an odd number of
+ * 8-byte words per slot, so a warp's 8-byte accesses to one field of 32
+ * slots are free of bank conflicts. */
+struct __align__(8) PathSlot {
+  Path p;
+  uint32_t pad[2];
+};
+static_assert(sizeof(PathSlot) % 16 == 8, "odd number of 8-byte words per slot");
+
+/* Shared-memory bytes of the path slots of a block (16-byte rounded) */
+__host__ __device__ constexpr size_t
+path_slots_bytes(uint32_t threads)
+{
+  return ((size_t)threads * sizeof(PathSlot) + 15) & ~(size_t)15;
+}
+
+/* Where the persistent kernel keeps a lane's path.  LW-only launches keep it
+ * in shared memory: with the path out of the registers the kernel needs ~156
+ * of them instead of 216, so 12 warps fit on an SM instead of 8, and LW
+ * walks are short enough that the shared-memory latency of each field access
+ * costs less than the occupancy gains (1149 against 919 Mrealisations/s on
+ * the LW flux map).  Shortwave walks are long and touch the path state
+ * between every dependent load: they keep it in registers (in shared memory
+ * the SW image ran 23 % slower). */
+__host__ __device__ constexpr bool
+persistent_smem_paths(unsigned v)
+{
+  return (v & HV_SW) == 0;
+}
+
 __device__ __forceinline__ void
 tables_to_smem(hg::PTables& T, unsigned char* smem)
 {
