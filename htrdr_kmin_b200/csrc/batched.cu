@@ -438,16 +438,18 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_maps_batched(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuning,
                             htrdr_gpu_stats* stats)
-{
+try {
   return batched_impl(items, n, tuning, stats, true);
 }
+HG_API_CATCH("htrdr_gpu_draw_maps_batched")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_maps_batched_device(htrdr_gpu_batch_item* items, size_t n,
                                    const htrdr_gpu_tuning* tuning, htrdr_gpu_stats* stats)
-{
+try {
   return batched_impl(items, n, tuning, stats, false);
 }
+HG_API_CATCH("htrdr_gpu_draw_maps_batched_device")
 
 /* Autotuner: times every candidate -- persistent megakernel (block size x
  * queue chunk x regroup period) and wavefront (tail threshold x regroup
@@ -456,7 +458,7 @@ htrdr_gpu_draw_maps_batched_device(htrdr_gpu_batch_item* items, size_t n,
  * tuning. */
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best, double* best_ms)
-{
+try {
   if(!items || !n || !best) return HTRDR_GPU_RES_BAD_ARG;
   static const uint32_t blocks[] = {96, 128, 256}; /* 96: 3 blocks of 3 warps fill 9 warps at 216 registers */
   static const uint32_t chunks[] = {1, 4};
@@ -498,6 +500,7 @@ htrdr_gpu_autotune(htrdr_gpu_batch_item* items, size_t n, htrdr_gpu_tuning* best
   if(best_ms) *best_ms = best_t;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_autotune")
 
 /*******************************************************************************
  * Reusable batch: the whole launch sequence (clear, persistent kernel,
@@ -531,7 +534,7 @@ htrdr_gpu_batch_release(htrdr_gpu_batch* b)
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_batch_create(const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuning,
                        htrdr_gpu_batch** out)
-{
+try {
   if(!items || !n || !out) return HTRDR_GPU_RES_BAD_ARG;
   htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
   if(!tuning) tun.engine = HTRDR_GPU_ENGINE_PERSISTENT; /* a mode default may name the wavefront */
@@ -559,11 +562,12 @@ htrdr_gpu_batch_create(const htrdr_gpu_batch_item* items, size_t n, const htrdr_
   *out = b;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_batch_create")
 
 /* Replays the captured launch: the items' device buffers receive the maps. */
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_batch_run(htrdr_gpu_batch* b, htrdr_gpu_stats* stats)
-{
+try {
   if(!b) return HTRDR_GPU_RES_BAD_ARG;
   cudaSetDevice(b->plan.device);
   unsigned long long c[5] = {0, 0, 0, 0, 0};
@@ -579,3 +583,4 @@ htrdr_gpu_batch_run(htrdr_gpu_batch* b, htrdr_gpu_stats* stats)
   read_stats(c, k, t, 1 + b->items.size(), stats); /* persistent kernel + finalizes */
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_batch_run")

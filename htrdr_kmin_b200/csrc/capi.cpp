@@ -127,7 +127,7 @@ struct DevArr {
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_set_engine(htrdr_gpu_scene* scn, int engine, const htrdr_gpu_tuning* tuning)
-{
+try {
   if(!scn) return HTRDR_GPU_RES_BAD_ARG;
   if(engine != HTRDR_GPU_ENGINE_PERSISTENT && engine != HTRDR_GPU_ENGINE_PLAIN
   && engine != HTRDR_GPU_ENGINE_WAVEFRONT)
@@ -143,21 +143,24 @@ htrdr_gpu_scene_set_engine(htrdr_gpu_scene* scn, int engine, const htrdr_gpu_tun
   if(tuning) scn->tuning = *tuning;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_scene_set_engine")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_map(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
                    const htrdr_gpu_buffer_layout* layout, void* buffer, htrdr_gpu_stats* stats)
-{
+try {
   return draw_map_impl(scn, req, layout, buffer, true, stats);
 }
+HG_API_CATCH("htrdr_gpu_draw_map")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_map_device(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
                           const htrdr_gpu_buffer_layout* layout, void* device_buffer,
                           htrdr_gpu_stats* stats)
-{
+try {
   return draw_map_impl(scn, req, layout, device_buffer, false, stats);
 }
+HG_API_CATCH("htrdr_gpu_draw_map_device")
 
 static htrdr_gpu_res_T
 radiance_impl(htrdr_gpu_scene* scn, int lw, size_t n, const double* pos, const double* dir,
@@ -189,22 +192,24 @@ extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_radiance_sw(htrdr_gpu_scene* scn, size_t n, const double* pos, const double* dir,
                       const double* wlen, const uint32_t* iband, const uint32_t* iquad,
                       int cpnt_mask, uint32_t seed, double* out)
-{
+try {
   return radiance_impl(scn, 0, n, pos, dir, wlen, iband, iquad, cpnt_mask, seed, out);
 }
+HG_API_CATCH("htrdr_gpu_radiance_sw")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_radiance_lw(htrdr_gpu_scene* scn, size_t n, const double* pos, const double* dir,
                       const double* wlen, const uint32_t* iband, const uint32_t* iquad,
                       uint32_t seed, double* out)
-{
+try {
   return radiance_impl(scn, 1, n, pos, dir, wlen, iband, iquad, 0, seed, out);
 }
+HG_API_CATCH("htrdr_gpu_radiance_lw")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_realisation_weights(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
                               size_t pix_begin, size_t pix_end, double* weights)
-{
+try {
   if(!scn || !req || !weights || pix_end < pix_begin) return HTRDR_GPU_RES_BAD_ARG;
   if(pix_end > (size_t)req->width * req->height) return HTRDR_GPU_RES_BAD_ARG;
   if(!cuda_ok(cudaSetDevice(scn->device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
@@ -221,10 +226,11 @@ htrdr_gpu_realisation_weights(htrdr_gpu_scene* scn, const htrdr_gpu_request* req
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_realisation_weights")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_find_band(htrdr_gpu_scene* scn, size_t n, const double* wlen, uint32_t* out)
-{
+try {
   if(!scn || (n && (!wlen || !out))) return HTRDR_GPU_RES_BAD_ARG;
   if(!n) return HTRDR_GPU_RES_OK;
   cudaSetDevice(scn->device);
@@ -236,11 +242,12 @@ htrdr_gpu_find_band(htrdr_gpu_scene* scn, size_t n, const double* wlen, uint32_t
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_find_band")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_sample_quad(htrdr_gpu_scene* scn, size_t n, const double* r, const uint32_t* iband,
                       uint32_t* out)
-{
+try {
   if(!scn || (n && (!r || !iband || !out))) return HTRDR_GPU_RES_BAD_ARG;
   if(!n) return HTRDR_GPU_RES_OK;
   cudaSetDevice(scn->device);
@@ -252,11 +259,12 @@ htrdr_gpu_sample_quad(htrdr_gpu_scene* scn, size_t n, const double* r, const uin
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_sample_quad")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_locate_leaf(htrdr_gpu_scene* scn, uint32_t iband, uint32_t iquad, int prop, size_t n,
                       const uint32_t* cells, uint32_t* node, uint32_t* level)
-{
+try {
   if(!scn || !scn->d.has_cloud || iband >= scn->nbands || iquad >= scn->nquads[iband]
   || prop < 0 || prop > 2 || !(scn->props_mask & (1u << prop)))
     return HTRDR_GPU_RES_BAD_ARG;
@@ -270,12 +278,13 @@ htrdr_gpu_locate_leaf(htrdr_gpu_scene* scn, uint32_t iband, uint32_t iquad, int 
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_locate_leaf")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_ground_trace(htrdr_gpu_scene* scn, size_t n, const float* rays, const float* tmax,
                        const uint32_t* from_prim, const uint8_t* from_edge, uint32_t* prim,
                        float* dist)
-{
+try {
   if(!scn || !scn->d.g_ntris) return HTRDR_GPU_RES_BAD_ARG;
   if(n && (!rays || !tmax || !from_prim || !from_edge || !prim || !dist)) return HTRDR_GPU_RES_BAD_ARG;
   if(!n) return HTRDR_GPU_RES_OK;
@@ -292,12 +301,13 @@ htrdr_gpu_ground_trace(htrdr_gpu_scene* scn, size_t n, const float* rays, const 
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_ground_trace")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_sample_wavelength(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, int channel,
                             size_t n, const double* r0, const double* r1, uint32_t* cdf_band,
                             double* wlen, double* pdf)
-{
+try {
   if(!scn || !req || channel < 0 || channel > 2) return HTRDR_GPU_RES_BAD_ARG;
   cudaSetDevice(scn->device);
   DRequest R;
@@ -315,3 +325,4 @@ htrdr_gpu_sample_wavelength(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, 
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_sample_wavelength")

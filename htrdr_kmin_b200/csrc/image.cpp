@@ -79,7 +79,7 @@ d_at(const char* p)
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_write_image(int mode, const htrdr_gpu_buffer_layout* layout, const void* buffer,
                       const char* path, htrdr_gpu_map_summary* summary)
-{
+try {
   if(!layout || !buffer || !path) return HTRDR_GPU_RES_BAD_ARG;
   if(mode < HG_XWAVE_SW || mode > HG_FLUX_LW) return HTRDR_GPU_RES_BAD_ARG;
   if(layout->elmt_size != pixel_size(mode) || layout->pitch < layout->width * layout->elmt_size)
@@ -134,3 +134,4 @@ htrdr_gpu_write_image(int mode, const htrdr_gpu_buffer_layout* layout, const voi
   }
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_write_image")

@@ -4,7 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <exception>
 #include <functional>
+#include <new>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -19,6 +21,22 @@ namespace hg {
 
 void set_error(const std::string& msg);
 bool cuda_ok(cudaError_t e, const char* what);
+
+/* Handler of the function-try-block of every C entry point returning a
+ * res_T: no C++ exception crosses the C ABI (a host allocation that fails
+ * becomes RES_MEM_ERR with the error text set). */
+#define HG_API_CATCH(entry)                                                \
+  catch(const std::bad_alloc&) {                                           \
+    hg::set_error(std::string(entry) + ": out of host memory");            \
+    return HTRDR_GPU_RES_MEM_ERR;                                          \
+  } catch(const std::exception& ex) {                                      \
+    hg::set_error(std::string(entry) + ": " + ex.what());                  \
+    return HTRDR_GPU_RES_UNKNOWN_ERR;                                      \
+  } catch(...) {                                                           \
+    hg::set_error(std::string(entry) + ": unknown exception");             \
+    return HTRDR_GPU_RES_UNKNOWN_ERR;                                      \
+  }
+
 /* Kernel launches of the calling thread since the last take_launches() */
 void note_launches(uint64_t n);
 uint64_t take_launches();

@@ -90,7 +90,7 @@ using namespace hg;
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_map_noalloc(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
                            const htrdr_gpu_buffer_layout* layout, void* device_buffer)
-{
+try {
   if(!scn || !req || !layout || !device_buffer) return HTRDR_GPU_RES_BAD_ARG;
   if(req->mode < 0 || req->mode > 4 || !req->width || !req->height || !req->spp)
     return HTRDR_GPU_RES_BAD_ARG;
@@ -234,3 +234,4 @@ htrdr_gpu_draw_map_noalloc(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   ok = ok && cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   return ok ? HTRDR_GPU_RES_OK : HTRDR_GPU_RES_UNKNOWN_ERR;
 }
+HG_API_CATCH("htrdr_gpu_draw_map_noalloc")

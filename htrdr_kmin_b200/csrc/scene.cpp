@@ -554,6 +554,20 @@ cache_read(const char* path, uint64_t signature, uint32_t depth, uint32_t nq, ui
     set_error(std::string("octree cache `") + path + "' was built from other inputs");
     return false;
   }
+  /* the file holds exactly what the header announces (checked before any
+   * allocation sized from the header) */
+  const long here = std::ftell(f.get());
+  if(here < 0 || std::fseek(f.get(), 0, SEEK_END) != 0) {
+    set_error(std::string("octree cache `") + path + "': not seekable");
+    return false;
+  }
+  const long end = std::ftell(f.get());
+  const uint64_t tables = (uint64_t)nq * 3 * 16;
+  if(end < here || h.nodes > ((uint64_t)1 << 40) || (uint64_t)(end - here) != tables + h.nodes * 16
+  || std::fseek(f.get(), here, SEEK_SET) != 0) {
+    set_error(std::string("octree cache `") + path + "': size does not match its header");
+    return false;
+  }
   base.resize((size_t)nq * 3);
   count.resize((size_t)nq * 3);
   nodes.resize((size_t)h.nodes * 4);
@@ -610,20 +624,22 @@ htrdr_gpu_res_T scene_create(int device, const htrdr_gpu_scene_desc* desc, const
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_create(int device, const htrdr_gpu_scene_desc* desc, htrdr_gpu_scene** out)
-{
+try {
   return scene_create(device, desc, nullptr, out);
 }
+HG_API_CATCH("htrdr_gpu_scene_create")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_create_cached(int device, const htrdr_gpu_scene_desc* desc, const char* cache_path,
                               htrdr_gpu_scene** out)
-{
+try {
   if(!cache_path || !*cache_path) {
     set_error("no cache path");
     return HTRDR_GPU_RES_BAD_ARG;
   }
   return scene_create(device, desc, cache_path, out);
 }
+HG_API_CATCH("htrdr_gpu_scene_create_cached")
 
 namespace {
 
@@ -920,7 +936,7 @@ htrdr_gpu_scene_tree_depth(const htrdr_gpu_scene* scn) { return scn ? scn->depth
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_get_tree(const htrdr_gpu_scene* scn, uint32_t iband, uint32_t iquad, int prop,
                          void* nodes, size_t capacity, size_t* count)
-{
+try {
   if(!scn || !count || iband >= scn->nbands || iquad >= scn->nquads[iband] || prop < 0 || prop > 2)
     return HTRDR_GPU_RES_BAD_ARG;
   const size_t idx = ((size_t)scn->quad_off[iband] + iquad) * 3 + (size_t)prop;
@@ -933,3 +949,4 @@ htrdr_gpu_scene_get_tree(const htrdr_gpu_scene* scn, uint32_t iband, uint32_t iq
     return HTRDR_GPU_RES_UNKNOWN_ERR;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_scene_get_tree")

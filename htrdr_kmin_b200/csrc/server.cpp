@@ -692,7 +692,7 @@ htrdr_gpu_server::loop_wave()
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_create(const htrdr_gpu_server_config* cfg, htrdr_gpu_server** out)
-{
+try {
   if(!cfg || !out || !cfg->hbm_budget_bytes || !valid_tuning(cfg->tuning)) return HTRDR_GPU_RES_BAD_ARG;
   int ndev = 0;
   if(cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
@@ -720,11 +720,12 @@ htrdr_gpu_server_create(const htrdr_gpu_server_config* cfg, htrdr_gpu_server** o
   *out = s;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_server_create")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_submit(htrdr_gpu_server* s, htrdr_gpu_scene* scene, const htrdr_gpu_request* req,
                         const htrdr_gpu_buffer_layout* layout, void* host_buffer, uint64_t* ticket)
-{
+try {
   if(!s || !scene || !req || !layout || !host_buffer || !ticket) return HTRDR_GPU_RES_BAD_ARG;
   if(scene->device != s->cfg.device) return HTRDR_GPU_RES_BAD_ARG;
   if(layout->width != req->width || layout->height != req->height
@@ -755,10 +756,11 @@ htrdr_gpu_server_submit(htrdr_gpu_server* s, htrdr_gpu_scene* scene, const htrdr
   s->cv_work.notify_one();
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_server_submit")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_poll(htrdr_gpu_server* s, uint64_t ticket, int* done, htrdr_gpu_res_T* result)
-{
+try {
   if(!s || !done) return HTRDR_GPU_RES_BAD_ARG;
   std::lock_guard<std::mutex> lk(s->m);
   auto it = s->all.find(ticket);
@@ -767,10 +769,11 @@ htrdr_gpu_server_poll(htrdr_gpu_server* s, uint64_t ticket, int* done, htrdr_gpu
   if(result) *result = it->second->result;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_server_poll")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_wait(htrdr_gpu_server* s, uint64_t ticket, double timeout_s, htrdr_gpu_res_T* result)
-{
+try {
   if(!s) return HTRDR_GPU_RES_BAD_ARG;
   std::unique_lock<std::mutex> lk(s->m);
   auto it = s->all.find(ticket);
@@ -782,10 +785,11 @@ htrdr_gpu_server_wait(htrdr_gpu_server* s, uint64_t ticket, double timeout_s, ht
   if(result) *result = r->result;
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_server_wait")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_stats(htrdr_gpu_server* s, struct htrdr_gpu_server_stats* st)
-{
+try {
   if(!s || !st) return HTRDR_GPU_RES_BAD_ARG;
   std::lock_guard<std::mutex> lk(s->m);
   std::memset(st, 0, sizeof(*st));
@@ -810,6 +814,7 @@ htrdr_gpu_server_stats(htrdr_gpu_server* s, struct htrdr_gpu_server_stats* st)
   }
   return HTRDR_GPU_RES_OK;
 }
+HG_API_CATCH("htrdr_gpu_server_stats")
 
 extern "C" HTRDR_GPU_API void
 htrdr_gpu_server_release(htrdr_gpu_server* s)
