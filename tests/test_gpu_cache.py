@@ -87,3 +87,13 @@ def test_cache_host_and_gpu_builders(gpu_lib, tmp_path):
     b = gpu_lib.GpuScene(sc, 0b111, cache_path=p_host)
     for x, y in zip(_trees(a, sc), _trees(b, sc)):
         np.testing.assert_array_equal(x, y)
+
+
+def test_cache_truncated(gpu_lib, tmp_path):
+    sc, _ = _scene()
+    path = tmp_path / "octrees.cache"
+    gpu_lib.GpuScene(sc, 0b100, cache_path=str(path))
+    data = path.read_bytes()
+    path.write_bytes(data[:-16])
+    with pytest.raises(gpu_lib.HtrdrError, match="size does not match"):
+        gpu_lib.GpuScene(sc, 0b100, cache_path=str(path))
