@@ -166,6 +166,40 @@ def parse_htrdr_obj(obj_text: str, materials: dict, sky_mtl: str = "air",
                       sky_mtl=mid.get(sky_mtl, NO_ID), mtl_names=tuple(names))
 
 
+def parse_htrdr_materials(text: str, brdf_tables: dict) -> dict:
+    """An htrdr-materials list (doc/htrdr-materials.5): one material per
+    line, `name none' for a semi-transparent material or `name path
+    temperature' for an opaque one, `#' starting a comment.  `brdf_tables'
+    maps each path to the BRDF table its mrumtl file holds, as
+    [(wavelength nm, "lambertian"|"specular", reflectivity), ...].  Returns
+    the materials dict that parse_htrdr_obj takes, in file order."""
+    mats = {}
+    for no, raw in enumerate(text.splitlines(), 1):
+        line = raw.split("#", 1)[0].strip()
+        if not line:
+            continue
+        tok = line.split()
+        name = tok[0]
+        if name in mats:
+            raise ValueError(f"line {no}: material `{name}' listed twice")
+        if len(tok) == 2 and tok[1] == "none":
+            mats[name] = None
+            continue
+        if len(tok) != 3:
+            raise ValueError(f"line {no}: expected `name none' or `name brdf-path temperature'")
+        path, temperature = tok[1], float(tok[2])
+        if not temperature >= 0.0:
+            raise ValueError(f"line {no}: invalid temperature `{tok[2]}'")
+        if path not in brdf_tables:
+            raise ValueError(f"line {no}: no BRDF table for `{path}'")
+        table = list(brdf_tables[path])
+        for wl, kind, refl in table:
+            if kind not in ("lambertian", "specular") or not 0.0 <= refl <= 1.0 or not wl > 0.0:
+                raise ValueError(f"line {no}: invalid BRDF entry ({wl}, {kind}, {refl}) in `{path}'")
+        mats[name] = (temperature, table)
+    return mats
+
+
 @dataclass
 class Scene:
     layer_z: np.ndarray  # float64 [nlayers+1]

@@ -188,3 +188,75 @@ def test_flux_probe_rejection_under_terrain(oracle_lib):
     w = O.OracleScene(sc).realisation_weights(rq, 0, rq.width * rq.height)
     rej = np.isnan(w).mean()
     assert 0.05 < rej < 0.95, rej
+
+
+def test_parse_htrdr_materials():
+    text = """# the example list of doc/htrdr-materials.5, with its BRDF tables
+grass   /opt/materials/A001.mrumtl 300
+sand    /opt/materials/B002.mrumtl 300   # trailing comment
+
+air     none
+"""
+    tables = {"/opt/materials/A001.mrumtl": [(400.0, "lambertian", 0.05), (700.0, "lambertian", 0.4)],
+              "/opt/materials/B002.mrumtl": [(550.0, "specular", 0.3)]}
+    mats = S.parse_htrdr_materials(text, tables)
+    assert list(mats) == ["grass", "sand", "air"]
+    assert mats["air"] is None
+    assert mats["grass"] == (300.0, tables["/opt/materials/A001.mrumtl"])
+    m = S.parse_htrdr_obj(FLAT_OBJ.replace("air:ground", "air:grass"), mats, sky_mtl="air")
+    np.testing.assert_array_equal(m.mtl_nbrdf, [2, 1, 0])
+    np.testing.assert_array_equal(m.mtl_temperature, [300.0, 300.0, -1.0])
+    assert m.sky_mtl == 2 and m.ifaces.tolist() == [[2, S.NO_ID, 0]]
+    for bad in ("grass /x 300\ngrass /x 300\n", "grass /x\n", "grass /missing 300\n",
+                "grass /x -4\n"):
+        with pytest.raises(ValueError):
+            S.parse_htrdr_materials(bad, {"/x": [(500.0, "lambertian", 0.1)]})
+    with pytest.raises(ValueError):
+        S.parse_htrdr_materials("g /x 300\n", {"/x": [(500.0, "glossy", 0.1)]})
+
+
+def test_htrdr_obj_doc_examples():
+    """The two examples of doc/htrdr-obj.5: a thin sheet of paper between
+    air and concrete, and a wooden cube against a brick along Z."""
+    paper = """v -1.0  -1.0  0
+v -1.0   1.0  0
+v  1.0  -1.0  0
+v  1.0   1.0  0
+
+usemtl air:paper:concrete
+f 1 2 3
+f 3 2 4
+"""
+    lam = (300.0, [(500.0, "lambertian", 0.5)])
+    m = S.parse_htrdr_obj(paper, {"air": None, "paper": lam, "concrete": lam})
+    assert m.ifaces.tolist() == [[0, 1, 2]] and m.tri_iface.tolist() == [0, 0]
+    v = m.verts[m.tris].astype(np.float64)
+    N = np.cross(v[:, 2] - v[:, 0], v[:, 1] - v[:, 0])
+    assert np.all(N[:, 2] > 0)  # vertices clockwise seen from +z: the front faces +z
+    cube = "\n".join(f"v {x} {y} {z}" for z in (0, 1) for y in (0, 1) for x in (0, 1)) + """
+usemtl wood:air
+f 1 3 2
+f 2 3 4
+f 1 5 3
+f 3 5 7
+f 5 6 7
+f 7 6 8
+f 4 8 2
+f 2 8 6
+
+usemtl wood:brick
+f 3 7 4
+f 4 7 8
+f 1 2 5
+f 5 2 6
+"""
+    m = S.parse_htrdr_obj(cube, {"wood": lam, "air": None, "brick": lam}, sky_mtl="air")
+    assert m.tris.shape == (12, 3) and m.verts.shape == (8, 3)
+    assert m.ifaces.tolist() == [[0, S.NO_ID, 1], [0, S.NO_ID, 2]]
+    assert m.tri_iface.tolist() == [0] * 8 + [1] * 4
+    # every face's front side (the wood) is inside the cube: the normal
+    # (v2 - v0) x (v1 - v0) of the clockwise convention points inwards
+    v = m.verts[m.tris].astype(np.float64)
+    N = np.cross(v[:, 2] - v[:, 0], v[:, 1] - v[:, 0])
+    out = v.mean(axis=1) - 0.5
+    assert np.all(np.einsum("ij,ij->i", N, out) < 0)
