@@ -165,3 +165,24 @@ def test_graph_batch_replay(gpu_lib, mix):
             got = np.frombuffer(b.cpu().numpy().tobytes(), dtype=api.pixel_dtype(r.mode)).reshape(r.height, r.width)
             _cmp(got, gs.draw_map(r)[0], r.mode)
     api.lib().htrdr_gpu_batch_release(h)
+
+
+@pytest.mark.parametrize("name,slots,tail", ENGINES[:2])
+def test_server_kinds_change(gpu_lib, mix, name, slots, tail):
+    """A server that has seen only longwave requests (LW-only kernel variants;
+    on the persistent engine, the variant with its paths in shared memory)
+    then admits shortwave and CIE ones: every map still equals its map drawn
+    alone."""
+    api = gpu_lib
+    lw = [(gs, r) for gs, r in mix if r.mode == S.MODE_FLUX_LW]
+    sw = [(gs, r) for gs, r in mix if r.mode != S.MODE_FLUX_LW]
+    assert lw and sw
+    srv = api.Server(round_target_ms=2.0, round_realisations=4096,
+                     tuning=_tuning(api, _engine(api, name), slots, tail))
+    first = [srv.submit(gs, r) for gs, r in lw]
+    out1 = [srv.wait(t, WAIT_S) for t in first]
+    second = [srv.submit(gs, r) for gs, r in sw + lw[:1]]
+    out2 = [srv.wait(t, WAIT_S) for t in second]
+    srv.close()
+    for (gs, r), got in zip(lw + sw + lw[:1], out1 + out2):
+        _cmp(got, gs.draw_map(r)[0], r.mode)
