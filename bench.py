@@ -37,6 +37,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -112,18 +113,59 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: a
+    thread reading NVML every 2 ms (the timed region of a few steps lasts tens
+    of milliseconds) and nvidia-smi every 100 ms.  Read-only queries; nothing
+    about the GPU's settings is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.path = None
+        self.nvml = None          # (module, handle) when NVML answers
+        self.nvml_samples = []    # (sm MHz, reasons bitmask)
+        self.nvml_max = None
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _nvml_open(self):
+        try:
+            import pynvml as N
+            import torch
+            N.nvmlInit()
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            try:
+                h = N.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                h = N.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml_max = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            self.nvml = (N, h)
+        except Exception:
+            self.nvml = None
+
+    def _nvml_loop(self):
+        N, h = self.nvml
+        reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            getattr(N, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        while not self._stop.is_set():
+            try:
+                self.nvml_samples.append((float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)),
+                                          int(reasons(h))))
+            except Exception:
+                return
+            self._stop.wait(0.002)
 
     def __enter__(self):
+        self._nvml_open()
+        if self.nvml is not None:
+            self._thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self._thread.start()
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -136,6 +178,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -143,25 +188,38 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
+    def _nvml_reason_names(self, mask: int):
+        N = self.nvml[0]
+        bits = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+                "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+                "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+                "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+        return {nm for nm, attr in bits.items() if mask & int(getattr(N, attr, 0))}
+
     def summary(self):
-        if self.proc is None or not self.path:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as f:
-            for line in f:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    smax = float(parts[2])
-                except ValueError:
-                    continue
-                for nm, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(nm)
-        os.unlink(self.path)
+        if self.nvml is not None:
+            for mhz, mask in self.nvml_samples:
+                sm.append(mhz)
+                reasons |= self._nvml_reason_names(mask)
+            smax = self.nvml_max
+        if self.proc is not None and self.path:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        smax = float(parts[2])
+                    except ValueError:
+                        continue
+                    for nm, v in zip(self.REASONS, parts[5:9]):
+                        if v.lower().startswith("active"):
+                            reasons.add(nm)
+            os.unlink(self.path)
+        if not sm and smax is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
