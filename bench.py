@@ -114,9 +114,10 @@ def peaks():
 
 class ClockSampler:
     """SM clocks and throttle reasons sampled during the timed region: a
-    thread reading NVML every 2 ms (the timed region of a few steps lasts tens
+    thread reading NVML every 5 ms (the timed region of a few steps lasts tens
     of milliseconds) and nvidia-smi every 100 ms.  Read-only queries; nothing
-    about the GPU's settings is changed."""
+    about the GPU's settings is changed.  `window_ms' is the wall time the
+    samples cover."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -132,6 +133,7 @@ class ClockSampler:
         self.nvml_max = None
         self._stop = threading.Event()
         self._thread = None
+        self.window = [0.0, 0.0]
 
     def _nvml_open(self):
         try:
@@ -159,10 +161,11 @@ class ClockSampler:
                                           int(reasons(h))))
             except Exception:
                 return
-            self._stop.wait(0.002)
+            time.sleep(0.005)
 
     def __enter__(self):
         self._nvml_open()
+        self.window[0] = time.perf_counter()
         if self.nvml is not None:
             self._thread = threading.Thread(target=self._nvml_loop, daemon=True)
             self._thread.start()
@@ -178,6 +181,7 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        self.window[1] = time.perf_counter()
         self._stop.set()
         if self._thread is not None:
             self._thread.join(timeout=5)
@@ -221,7 +225,8 @@ class ClockSampler:
         if not sm and smax is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window_ms": 1e3 * (self.window[1] - self.window[0])}
 
 
 def workload(name: str):
