@@ -37,11 +37,15 @@ enum { HG_XWAVE_SW = 0, HG_XWAVE_LW = 1, HG_IMAGE_CIE = 2, HG_FLUX_SW = 3, HG_FL
  * realisation (never a stuck one). */
 enum : uint32_t { HV_MESH = 1u, HV_SW = 2u, HV_LW = 4u, HV_ALL = 7u };
 
+/* Internal modes of the batched radiance entry points */
+#define HG_RAD_SW 5
+#define HG_RAD_LW 6
+
 /* Spectral kind of an output mode (HV_SW or HV_LW) */
 static inline uint32_t
 hv_kind(int mode)
 {
-  return (mode == HG_XWAVE_LW || mode == HG_FLUX_LW) ? HV_LW : HV_SW;
+  return (mode == HG_XWAVE_LW || mode == HG_FLUX_LW || mode == HG_RAD_LW) ? HV_LW : HV_SW;
 }
 
 /* A variant from the launch's mesh flag and kinds (no kind: both) */

@@ -444,9 +444,6 @@ enum {
   ST_SW_ABS_END, ST_SW_NEE_END, ST_LW_WALK, ST_LW_END, ST_RAD_END, ST_TRACE, ST_DONE
 };
 
-/* Internal modes for the batched radiance entry points */
-#define HG_RAD_SW 5
-#define HG_RAD_LW 6
 
 enum {
   PF_SURFACE = 1u << 0, PF_SPECULAR = 1u << 1, PF_PREV_GROUND = 1u << 2, PF_RAYLEIGH = 1u << 3,

@@ -157,7 +157,9 @@ htrdr_gpu_scene_create(int device, const struct htrdr_gpu_scene_desc* desc,
  * loaded instead of built, and optical_thickness and grid_max_definition
  * (-T, -V) are ignored; when it holds octrees of another medium the call
  * fails with RES_BAD_ARG; when it does not exist the octrees are built and
- * written to it.  The file stores 16-byte nodes in the device layout. */
+ * written to it.  The file stores 16-byte nodes in the device layout.  A
+ * clear sky (no cloud grid) has no octrees: the cache is then neither read
+ * nor written. */
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_scene_create_cached(int device, const struct htrdr_gpu_scene_desc* desc,
                               const char* cache_path, struct htrdr_gpu_scene** scene);
