@@ -141,8 +141,9 @@ def _three_sigma(bufs_a, bufs_b, keys):
     return np.concatenate(zs)
 
 
-@pytest.mark.parametrize("lw", [False, True], ids=["sw", "lw"])
-def test_flat_mesh_matches_plane(oracle_lib, lw):
+@pytest.mark.parametrize("lw,specular", [(False, False), (True, False), (False, True)],
+                         ids=["sw", "lw", "sw_specular"])
+def test_flat_mesh_matches_plane(oracle_lib, lw, specular):
     """A flat repeated mesh = the plane ground (same BRDF, temperature)."""
     O = oracle_lib
     if lw:
@@ -161,7 +162,9 @@ def test_flat_mesh_matches_plane(oracle_lib, lw):
                        wlen_range=(550.0, 550.0), cam_pos=(100.0, 100.0, 500.0),
                        cam_tgt=(400.0, 600.0, 0.0), cam_up=(0.0, 0.0, 1.0), fov_deg=60.0,
                        seed=7)
-        mesh = flat_mesh(refl=0.4, T=288.0)
+        mesh = flat_mesh(refl=0.4, T=288.0, specular=specular)
+        if specular:
+            sc.ground_brdf = S.BRDF_SPECULAR
     plane = O.OracleScene(sc)
     sm = _flat_scene(mesh)
     sm.layer_T, sm.gas_ka, sm.gas_ks = sc.layer_T, sc.gas_ka, sc.gas_ks
