@@ -110,3 +110,22 @@ def test_struct_layout_matches_header(tmp_path, struct, mirror):
                                           text=True).stdout.split()]
     assert out[0] == C.sizeof(cls)
     assert out[1:] == [getattr(cls, n).offset for n in names]
+
+
+def test_c_caller(tmp_path):
+    """A strict-C99 caller (tests/c/abi_caller.c) compiles against the header
+    with every warning as an error, links the library and checks the calls
+    that need no device."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    lib = build.build()
+    exe = tmp_path / "abi_caller"
+    libdir = os.path.dirname(lib)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Wpedantic", "-Werror",
+                    "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "abi_caller.c"),
+                    "-L", libdir, "-lhtrdr_gpu", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe), str(tmp_path / "map.txt")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "abi_caller ok" in r.stdout
