@@ -107,3 +107,19 @@ def test_image_writer_rejects_bad_arguments(tmp_path):
     with pytest.raises(api.HtrdrError) as e:
         api.write_image(S.MODE_XWAVE_SW, buf, os.path.join(str(tmp_path), "no", "such", "dir.txt"))
     assert e.value.code == api.RES_IO_ERR
+
+
+@pytest.mark.parametrize("name", ["xwave_sw", "xwave_lw", "image_cie", "flux_sw", "flux_lw"])
+def test_image_golden_fixtures(tmp_path, name):
+    """The writer's output for the committed pixel buffers equals the
+    committed text (tests/golden, made by make_image_golden.py)."""
+    build.build()
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    mode = {"xwave_sw": S.MODE_XWAVE_SW, "xwave_lw": S.MODE_XWAVE_LW, "image_cie": S.MODE_IMAGE_CIE,
+            "flux_sw": S.MODE_FLUX_SW, "flux_lw": S.MODE_FLUX_LW}[name]
+    buf = np.load(os.path.join(golden, f"image_{name}.npy"))
+    assert buf.dtype == api.pixel_dtype(mode)
+    path = str(tmp_path / "map.txt")
+    api.write_image(mode, buf, path)
+    with open(path) as f, open(os.path.join(golden, f"image_{name}.txt")) as g:
+        assert f.read() == g.read()
