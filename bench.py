@@ -185,6 +185,11 @@ class ClockSampler:
         self._stop.set()
         if self._thread is not None:
             self._thread.join(timeout=5)
+        if self.nvml is not None:
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
