@@ -263,3 +263,21 @@ f 5 2 6
     N = np.cross(v[:, 2] - v[:, 0], v[:, 1] - v[:, 0])
     out = v.mean(axis=1) - 0.5
     assert np.all(np.einsum("ij,ij->i", N, out) < 0)
+
+
+def test_black_mesh_emits_planck(oracle_lib):
+    """Closed form on the mesh: under a transparent atmosphere a camera that
+    sees only a black (reflectivity 0) repeated mesh at temperature T
+    measures B(lambda, T) exactly, every realisation."""
+    O = oracle_lib
+    T = 300.0
+    sc = S.homogeneous_slab(k_abs=1e-30, k_sca=0.0, top=2000.0, temperature=250.0,
+                            band=(9500.0, 10500.0))
+    sc.ground_mesh = flat_mesh(refl=0.0, T=T, repeat=True)
+    rq = S.Request(mode=S.MODE_XWAVE_LW, width=4, height=4, spp=8, wlen_range=(10000.0, 10000.0),
+                   ref_temperature=T, cam_pos=(200.0, 300.0, 500.0), cam_tgt=(250.0, 350.0, 0.0),
+                   cam_up=(0.0, 1.0, 0.0), fov_deg=30.0, seed=3)
+    w = O.OracleScene(sc).realisation_weights(rq, 0, 16)
+    B = O.lib().ora_planck_monochromatic(10000e-9, T)
+    # weight = radiance / pdf(lambda) with a Dirac spectral domain: pdf 1 per nm
+    np.testing.assert_allclose(w, B * 1e-9, rtol=1e-9)
