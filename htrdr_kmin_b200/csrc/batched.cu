@@ -243,9 +243,7 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
       return HTRDR_GPU_RES_BAD_ARG;
     const htrdr_gpu_buffer_layout& L = items[i].layout;
     const htrdr_gpu_request& q = items[i].req;
-    if(L.width != q.width || L.height != q.height || L.elmt_size != pixel_size(q.mode)
-    || L.pitch < L.width * L.elmt_size)
-      return HTRDR_GPU_RES_BAD_ARG;
+    if(check_layout(&q, &L) != HTRDR_GPU_RES_OK) return HTRDR_GPU_RES_BAD_ARG;
   }
   if(!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
   P.device = device;

@@ -102,6 +102,9 @@ Sampler* scene_sampler(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, htrdr
 /* Fill the device view of a request */
 htrdr_gpu_res_T make_drequest(htrdr_gpu_scene* scn, const htrdr_gpu_request* req, DRequest* out);
 uint32_t pixel_size(int mode);
+/* Output layout of a request: the buffer checks of htrdr_buffer_layout and the
+ * mode's pixel struct; every draw_map entry point applies it */
+htrdr_gpu_res_T check_layout(const htrdr_gpu_request* req, const htrdr_gpu_buffer_layout* layout);
 
 /* Octree build on the host, bit-exact definition shared with the oracle.
  * Writes nodes[4*i..] = {kmin bits, kmax bits, child, 0}. */

@@ -94,9 +94,7 @@ try {
   if(!scn || !req || !layout || !device_buffer) return HTRDR_GPU_RES_BAD_ARG;
   if(req->mode < 0 || req->mode > 4 || !req->width || !req->height || !req->spp)
     return HTRDR_GPU_RES_BAD_ARG;
-  if(layout->width != req->width || layout->height != req->height
-  || layout->elmt_size != pixel_size(req->mode) || layout->pitch < layout->width * layout->elmt_size)
-    return HTRDR_GPU_RES_BAD_ARG;
+  if(check_layout(req, layout) != HTRDR_GPU_RES_OK) return HTRDR_GPU_RES_BAD_ARG;
   if(req->wlen_range[0] > req->wlen_range[1]) return HTRDR_GPU_RES_BAD_ARG;
   const bool lw = req->mode == HG_XWAVE_LW || req->mode == HG_FLUX_LW;
   const bool cie = req->mode == HG_IMAGE_CIE;

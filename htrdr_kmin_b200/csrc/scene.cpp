@@ -254,6 +254,20 @@ pixel_size(int mode)
   return mode == HG_IMAGE_CIE ? 80u : 64u;
 }
 
+htrdr_gpu_res_T
+check_layout(const htrdr_gpu_request* req, const htrdr_gpu_buffer_layout* layout)
+{
+  /* htrdr_buffer_layout_check + the pixel format of atmosphere_get_pixel_format
+   * (src/atmosphere/htrdr_atmosphere.c:482-509) */
+  if(!layout || !req) return HTRDR_GPU_RES_BAD_ARG;
+  if(layout->width != req->width || layout->height != req->height) return HTRDR_GPU_RES_BAD_ARG;
+  if(layout->elmt_size != pixel_size(req->mode)) return HTRDR_GPU_RES_BAD_ARG;
+  if(layout->pitch < layout->width * layout->elmt_size) return HTRDR_GPU_RES_BAD_ARG;
+  if(layout->alignment && (layout->alignment & (layout->alignment - 1))) return HTRDR_GPU_RES_BAD_ARG;
+  if(layout->alignment > 16) return HTRDR_GPU_RES_BAD_ARG;
+  return HTRDR_GPU_RES_OK;
+}
+
 static void
 onb_d(const double n[3], double b1[3], double b2[3])
 {

@@ -728,9 +728,7 @@ htrdr_gpu_server_submit(htrdr_gpu_server* s, htrdr_gpu_scene* scene, const htrdr
 try {
   if(!s || !scene || !req || !layout || !host_buffer || !ticket) return HTRDR_GPU_RES_BAD_ARG;
   if(scene->device != s->cfg.device) return HTRDR_GPU_RES_BAD_ARG;
-  if(layout->width != req->width || layout->height != req->height
-  || layout->elmt_size != pixel_size(req->mode) || layout->pitch < layout->width * layout->elmt_size)
-    return HTRDR_GPU_RES_BAD_ARG;
+  if(check_layout(req, layout) != HTRDR_GPU_RES_OK) return HTRDR_GPU_RES_BAD_ARG;
   auto r = std::make_unique<SReq>();
   cudaSetDevice(scene->device);
   const htrdr_gpu_res_T res = make_drequest(scene, req, &r->dreq);

@@ -19,10 +19,18 @@ F64_WORDS = [0, 1, 4, 5]
 U64_WORDS = [2, 3, 6, 7]
 
 
+# Odd 32-bit multiplier (the golden-ratio Weyl increment): rank -> rank * K
+# is a bijection modulo 2^32, so the ranks of one job never share a seed.
+_RANK_STRIDE = 0x9E3779B9
+
+
 def rank_seed(seed: int, rank: int) -> int:
-    """Seed of a rank's random streams: distinct per rank, rank 0 keeps the
-    single-GPU streams."""
-    return (seed * 1000 + rank) & 0xFFFFFFFF
+    """Seed of a rank's random streams.  Rank 0 keeps the request's seed
+    (the single-GPU streams); rank r adds r times an odd constant modulo 2^32,
+    so two ranks of one job never draw the same streams for a request."""
+    if not 0 <= rank < (1 << 32):
+        raise ValueError(f"rank {rank} out of range")
+    return (seed + rank * _RANK_STRIDE) & 0xFFFFFFFF
 
 
 def reduce_flux_map(buf, dist, dst: int = 0) -> None:

@@ -444,7 +444,7 @@ def config_c2(scale: float = 1.0, spp: Optional[int] = None,
     ka, ks, w = gas_lw(layer_z, band_lo, band_hi, nquads, SEED_S1 + 7)
     nx, ny, nz = cloud_def
     lwc = lwc_lognormal((nz, ny, nx), SEED_S2 + 7)
-    sig, ssa, g = _cloud_optics(16, 0.5)
+    sig, ssa, g = _cloud_optics(16, 0.999)
     dz = 1000.0 / nz
     scene = Scene(layer_z=layer_z, layer_T=temperature_profile(layer_z), band_lo=band_lo,
                   band_hi=band_hi, nquads=nquads, quad_w=w, gas_ka=ka, gas_ks=ks,
@@ -509,7 +509,7 @@ def batched_scenes(scale: float = 1.0) -> List[Scene]:
         w = np.concatenate([w_s, w_l])
         lwc = lwc_power_law((nz, ny, nx), s)
         sig = np.full(8, SIGMA_EXT_CLOUD, dtype=np.float32)
-        ssa = np.array([0.999] * 4 + [0.5] * 4, dtype=np.float32)
+        ssa = np.full(8, 0.999, dtype=np.float32)  # the cloud recipe's albedo in every band
         g = np.full(8, 0.85, dtype=np.float32)
         cell = 6400.0 / max(nx, ny) if scale != 1.0 else 50.0
         dz = 1000.0 / nz  # a 1 km thick cloud layer based at 1 km

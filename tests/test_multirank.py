@@ -76,5 +76,6 @@ def test_two_rank_flux_reduction(tmp_path):
 
 def test_rank_seeds_are_distinct():
     from htrdr_kmin_b200 import multigpu as M
-    seeds = {M.rank_seed(2, r) for r in range(8)}
-    assert len(seeds) == 8 and M.rank_seed(2, 0) == 2000
+    seeds = {M.rank_seed(2, r) for r in range(4096)}
+    assert len(seeds) == 4096 and M.rank_seed(2, 0) == 2
+    assert all(0 <= s < (1 << 32) for s in seeds)

@@ -84,3 +84,41 @@ def test_noalloc_rejects_oversize_requests(gpu_lib):
     assert _noalloc(api, gs, big, out.data_ptr()) == api.RES_BAD_ARG
     assert b"65536" in api.lib().htrdr_gpu_last_error()
     gs.close()
+
+
+def test_noalloc_takes_no_device_memory(gpu_lib):
+    """The entry point's contract: after the first call on a device (which
+    looks up the static arrays and may load the kernels), further calls leave
+    the device's free memory unchanged."""
+    import torch
+    api = gpu_lib
+    scene, req = S.config_c2(scale=32 / 128, spp=4, cloud_def=(16, 16, 8))
+    gs = api.GpuScene(scene, 0b100)
+    out = _device_buffer(req, api)
+    assert _noalloc(api, gs, req, out.data_ptr()) == api.RES_OK
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        assert _noalloc(api, gs, req, out.data_ptr()) == api.RES_OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    gs.close()
+
+
+def test_noalloc_rejects_the_layouts_draw_map_device_rejects(gpu_lib):
+    api = gpu_lib
+    scene, req = S.config_c2(scale=4 / 128, spp=1, cloud_def=(4, 4, 2))
+    gs = api.GpuScene(scene, 0b100)
+    out = _device_buffer(req, api)
+    L = api.lib()
+    fn = L.htrdr_gpu_draw_map_noalloc
+    fn.argtypes = [C.c_void_p, C.POINTER(api.Request), C.POINTER(api.BufferLayout), C.c_void_p]
+    r = api.to_request(req)
+    for alignment in (3, 32):  # not a power of two; above 16
+        lay = api.layout_for(req)
+        lay.alignment = alignment
+        assert fn(gs.handle, C.byref(r), C.byref(lay), C.c_void_p(out.data_ptr())) == api.RES_BAD_ARG
+        st = api.Stats()
+        assert L.htrdr_gpu_draw_map_device(gs.handle, C.byref(r), C.byref(lay),
+                                           C.c_void_p(out.data_ptr()), C.byref(st)) == api.RES_BAD_ARG
+    gs.close()
