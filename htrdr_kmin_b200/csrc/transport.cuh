@@ -373,8 +373,9 @@ ground_query(const DScene& S, float3 o, float3 d, float r1, bool prev, uint32_t 
  * type and reflectivity and the temperature.  On the mesh, the material of
  * the hit side's interface and the BRDF tabulated at the wavelength, chosen
  * with one transport canonical as htrdr_mtl_create_bsdf does
- * (src/core/htrdr_materials.c:414-463); on the plane, its constants and no
- * draw.  A side without a BRDF reflects nothing. */
+ * (src/core/htrdr_materials.c:414-463); on the plane, its constants, the
+ * canonical being drawn all the same (htrdr_mtl_create_bsdf draws it whatever
+ * the material's BRDF count, :428).  A side without a BRDF reflects nothing. */
 struct SurfProps {
   float3 N;
   float refl, T;
@@ -387,6 +388,7 @@ surface_props(const DScene& S, Rng& rng, float3 dir, uint32_t prim, float3 ng, d
 {
   SurfProps s;
   if(!(V & HV_MESH) || !S.g_ntris) {
+    (void)rng.uf();
     s.N = make_float3(0.f, 0.f, 1.f);
     s.refl = S.ground_refl;
     s.specular = S.ground_brdf == 1;

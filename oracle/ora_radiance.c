@@ -168,7 +168,9 @@ ground_query(const struct ora_scene* scn, const double o[3], const double d[3], 
  * temperature.  Mesh: the material of the hit side (htrdr_interface_fetch_hit_mtl)
  * and its BRDF at the wavelength, chosen with one transport canonical
  * (htrdr_mtl_create_bsdf); a side without a BRDF reflects nothing.  Plane:
- * its constants, no draw. */
+ * its constants; the canonical is drawn all the same, as
+ * htrdr_mtl_create_bsdf draws it whatever the material's BRDF count
+ * (src/core/htrdr_materials.c:428). */
 struct surf {
   double N[3];
   double refl, T;
@@ -183,6 +185,7 @@ surface_props(const struct ora_scene* scn, struct ora_rng* rng, const double dir
   uint32_t m, b;
   double r, n;
   if(!scn->g_ntris) {
+    (void)canonical(rng);
     s.N[0] = 0; s.N[1] = 0; s.N[2] = 1;
     s.refl = scn->ground_reflectivity;
     s.specular = scn->ground_brdf == 1;
@@ -229,7 +232,9 @@ in_solar_cone(const struct ora_scene* scn, const double d[3])
 
 /* Flat ground z = 0 (htrdr_atmosphere_ground_trace_ray with the self-hit
  * filter of src/core/htrdr_geometry.c:118-150: hits strictly inside the range
- * and not on the primitive the ray starts from).  Returns the distance or -1. */
+ * and not on the primitive the ray starts from).  Returns the distance or -1;
+ * the distance is rounded to single precision, the precision of the star-3d
+ * hit record the reference reads it from (s3d_hit.distance). */
 double
 ora_ground_trace(const struct ora_scene* scn, const double o[3], const double d[3],
                  double r0, double r1, int prev_ground)
@@ -238,7 +243,7 @@ ora_ground_trace(const struct ora_scene* scn, const double o[3], const double d[
   if(!scn->has_ground || prev_ground || d[2] == 0.0) return -1;
   t = -o[2] / d[2];
   if(t <= r0 || t >= r1) return -1;
-  return t;
+  return (double)(float)t;
 }
 
 /*******************************************************************************
@@ -410,7 +415,8 @@ ora_radiance_sw(const struct ora_scene* scn, struct ora_rng* rng, int cpnt_mask,
 
     wo[0] = -dir[0]; wo[1] = -dir[1]; wo[2] = -dir[2];
     surface = !svx_hit;
-    if(surface) sc.traversal_dst = ground_dst;
+    /* a surface event lies where the traversal ended (..._sw.c:382-385):
+     * the ground distance, or the column's bottom if that is nearer */
     for(i = 0; i < 3; ++i) pos_next[i] = pos[i] + dir[i] * sc.traversal_dst;
     prev_ground = surface;
     if(surface) { prev_prim = gh.prim; prev_edge = ora_on_edge(gh.u, gh.v) && scn->g_ntris; }
@@ -501,7 +507,6 @@ ora_radiance_lw(const struct ora_scene* scn, struct ora_rng* rng, const double p
     svx_hit = ora_trace_ray(scn, band, q, ORA_KEXT, pos, dir, range, lw_hit_filter, &c, cnt, &hit);
 
     if(ground_dst < 0 && !svx_hit) { w = 0; break; }
-    if(!svx_hit) c.traversal_dst = ground_dst;
     for(i = 0; i < 3; ++i) pos_next[i] = pos[i] + dir[i] * c.traversal_dst;
 
     if(svx_hit && c.event == 0) { /* absorption: emission at the local temperature */

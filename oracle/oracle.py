@@ -2,9 +2,9 @@
 
 TEST INFRASTRUCTURE ONLY: a plain-C, FP64-transport restatement of the
 reference's atmosphere path, used by tests/, the smoke check and the CPU
-baseline of bench.py.  PARITY UNPINNED against reference outputs (none
-exist for this path, and the reference cannot be built here); pinned instead
-against closed-form FP64 solutions in tests/test_oracle_pins.py.
+baseline of bench.py.  Pinned to the reference's own code compiled unmodified
+(oracle/reference.py, tests/test_reference_pin.py: equal realisation by
+realisation) and to closed-form FP64 solutions (tests/test_oracle_pins.py).
 """
 from __future__ import annotations
 
@@ -155,53 +155,61 @@ def _p(a: np.ndarray, ct):
     return a.ctypes.data_as(C.POINTER(ct))
 
 
+def scene_desc(scene, props_mask: int = 0b111):
+    """The C description of a scene (SceneDesc) and the arrays it points to,
+    which must stay alive while the description is in use."""
+    scene.validate()
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a
+
+    d = SceneDesc()
+    d.nlayers = scene.nlayers
+    d.layer_z = _p(arr(scene.layer_z, np.float64), C.c_double)
+    d.layer_T = _p(arr(scene.layer_T, np.float32), C.c_float)
+    d.nbands = scene.nbands
+    d.band_lo = _p(arr(scene.band_lo, np.float64), C.c_double)
+    d.band_hi = _p(arr(scene.band_hi, np.float64), C.c_double)
+    d.nquads = _p(arr(scene.nquads, np.uint32), C.c_uint32)
+    d.quad_w = _p(arr(scene.quad_w, np.float64), C.c_double)
+    d.gas_ka = _p(arr(scene.gas_ka, np.float32), C.c_float)
+    d.gas_ks = _p(arr(scene.gas_ks, np.float32), C.c_float)
+    cd = scene.cloud_def
+    for i in range(3):
+        d.cloud_def[i] = cd[i]
+        d.cloud_lower[i] = scene.cloud_lower[i]
+        d.cloud_cell[i] = scene.cloud_cell[i]
+        d.grid_max_definition[i] = scene.grid_max_definition[i]
+    if scene.cloud_lwc is not None:
+        d.cloud_lwc = _p(arr(scene.cloud_lwc, np.float32), C.c_float)
+    nb = scene.nbands
+    zeros = np.zeros(nb)
+    d.cloud_sigma_ext = _p(arr(scene.cloud_sigma_ext if scene.cloud_sigma_ext is not None else zeros, np.float32), C.c_float)
+    d.cloud_ssa = _p(arr(scene.cloud_ssa if scene.cloud_ssa is not None else zeros, np.float32), C.c_float)
+    d.cloud_g = _p(arr(scene.cloud_g if scene.cloud_g is not None else zeros, np.float32), C.c_float)
+    d.repeat_clouds = int(scene.repeat_clouds)
+    d.optical_thickness = scene.optical_thickness
+    d.has_ground = int(scene.has_ground)
+    d.ground_brdf = int(scene.ground_brdf)
+    d.ground_reflectivity = scene.ground_reflectivity
+    d.ground_temperature = scene.ground_temperature
+    d.sun_azimuth = scene.sun_azimuth
+    d.sun_elevation = scene.sun_elevation
+    d.props_mask = props_mask
+    if scene.ground_mesh is not None:
+        scene.ground_mesh.fill_desc(d, keep)
+    return d, keep
+
+
 class OracleScene:
     """A scene loaded into the oracle (majorant octrees built on creation)."""
 
     def __init__(self, scene, props_mask: int = 0b111):
-        scene.validate()
+        d, self._keep = scene_desc(scene, props_mask)
         self.scene = scene
-        keep = []
-
-        def arr(a, dt):
-            a = np.ascontiguousarray(a, dtype=dt)
-            keep.append(a)
-            return a
-
-        d = SceneDesc()
-        d.nlayers = scene.nlayers
-        d.layer_z = _p(arr(scene.layer_z, np.float64), C.c_double)
-        d.layer_T = _p(arr(scene.layer_T, np.float32), C.c_float)
-        d.nbands = scene.nbands
-        d.band_lo = _p(arr(scene.band_lo, np.float64), C.c_double)
-        d.band_hi = _p(arr(scene.band_hi, np.float64), C.c_double)
-        d.nquads = _p(arr(scene.nquads, np.uint32), C.c_uint32)
-        d.quad_w = _p(arr(scene.quad_w, np.float64), C.c_double)
-        d.gas_ka = _p(arr(scene.gas_ka, np.float32), C.c_float)
-        d.gas_ks = _p(arr(scene.gas_ks, np.float32), C.c_float)
-        cd = scene.cloud_def
-        for i in range(3):
-            d.cloud_def[i] = cd[i]
-            d.cloud_lower[i] = scene.cloud_lower[i]
-            d.cloud_cell[i] = scene.cloud_cell[i]
-            d.grid_max_definition[i] = scene.grid_max_definition[i]
-        if scene.cloud_lwc is not None:
-            d.cloud_lwc = _p(arr(scene.cloud_lwc, np.float32), C.c_float)
-        nb = scene.nbands
-        d.cloud_sigma_ext = _p(arr(scene.cloud_sigma_ext if scene.cloud_sigma_ext is not None else np.zeros(nb), np.float32), C.c_float)
-        d.cloud_ssa = _p(arr(scene.cloud_ssa if scene.cloud_ssa is not None else np.zeros(nb), np.float32), C.c_float)
-        d.cloud_g = _p(arr(scene.cloud_g if scene.cloud_g is not None else np.zeros(nb), np.float32), C.c_float)
-        d.repeat_clouds = int(scene.repeat_clouds)
-        d.optical_thickness = scene.optical_thickness
-        d.has_ground = int(scene.has_ground)
-        d.ground_brdf = int(scene.ground_brdf)
-        d.ground_reflectivity = scene.ground_reflectivity
-        d.ground_temperature = scene.ground_temperature
-        d.sun_azimuth = scene.sun_azimuth
-        d.sun_elevation = scene.sun_elevation
-        d.props_mask = props_mask
-        if scene.ground_mesh is not None:
-            scene.ground_mesh.fill_desc(d, keep)
         h = C.c_void_p()
         res = lib().ora_scene_create(C.byref(d), C.byref(h))
         if res != 0:

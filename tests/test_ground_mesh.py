@@ -5,10 +5,10 @@ queries and transport.
   front:back and front:thin:back groups, materials and BRDF tables;
 * ray queries on a flat quad against their closed-form answers: distance,
   the primitive left by the ray (self-hit), the range, the repeated tile;
-* a flat repeated mesh with one Lambertian material estimates the same
-  radiance and flux as the plane ground with the same reflectivity and
-  temperature (within 3 standard errors; the mesh draws one more canonical
-  per surface event to choose a BRDF, so streams are not matched).
+* a flat repeated mesh with one material gives the plane ground's weights
+  realisation by realisation (both draw the canonical that picks a BRDF at
+  every surface event, as htrdr_mtl_create_bsdf does; the hit distances are
+  FP32 on both) and so estimates the same radiance.
 """
 import math
 
@@ -170,6 +170,11 @@ def test_flat_mesh_matches_plane(oracle_lib, lw, specular):
     sm.layer_T, sm.gas_ka, sm.gas_ks = sc.layer_T, sc.gas_ka, sc.gas_ks
     sm.band_lo, sm.band_hi, sm.sun_elevation = sc.band_lo, sc.band_hi, sc.sun_elevation
     meshed = O.OracleScene(sm)
+    npix = rq.width * rq.height
+    wa = plane.realisation_weights(S.Request(**{**rq.__dict__, "spp": 200}), 0, npix)
+    wb = meshed.realisation_weights(S.Request(**{**rq.__dict__, "spp": 200}), 0, npix)
+    rel = np.abs(wa - wb) / np.maximum(np.abs(wa), 1e-300)
+    assert np.all(rel <= 1e-6), rel.max()  # same streams, same events
     a, _ = plane.draw_map(rq)
     b, _ = meshed.draw_map(rq)
     assert np.all(a["L"] > 0) and np.all(b["L"] > 0)
