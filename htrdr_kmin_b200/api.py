@@ -42,7 +42,9 @@ EXPORTED = [
     "htrdr_gpu_server_stats", "htrdr_gpu_server_release",
     "htrdr_gpu_default_tuning", "htrdr_gpu_version", "htrdr_gpu_device_count",
     "htrdr_gpu_last_error", "htrdr_gpu_scene_set_engine", "htrdr_gpu_mode_tuning",
-    "htrdr_gpu_write_image", "htrdr_gpu_ground_trace",
+    "htrdr_gpu_write_image", "htrdr_gpu_ground_trace", "htrdr_gpu_draw_map_noalloc",
+    "htrdr_gpu_draw_map_accum_device", "htrdr_gpu_finalize_device",
+    "htrdr_gpu_draw_maps_batched_accum_device",
 ]
 
 ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT = 0, 1, 2
@@ -185,6 +187,8 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_scene_get_tree.argtypes = [vp, u32, u32, i32, vp, sz, C.POINTER(C.c_size_t)]
     L.htrdr_gpu_draw_map.argtypes = [vp, C.POINTER(Request), C.POINTER(BufferLayout), vp, C.POINTER(Stats)]
     L.htrdr_gpu_draw_map_device.argtypes = [vp, C.POINTER(Request), C.POINTER(BufferLayout), vp, C.POINTER(Stats)]
+    L.htrdr_gpu_draw_map_accum_device.argtypes = [vp, C.POINTER(Request), vp, C.POINTER(Stats)]
+    L.htrdr_gpu_finalize_device.argtypes = [vp, C.POINTER(Request), vp, C.POINTER(BufferLayout), vp]
     L.htrdr_gpu_radiance_sw.argtypes = [vp, sz, dp, dp, dp, up, up, i32, u32, dp]
     L.htrdr_gpu_radiance_lw.argtypes = [vp, sz, dp, dp, dp, up, up, u32, dp]
     L.htrdr_gpu_realisation_weights.argtypes = [vp, C.POINTER(Request), sz, sz, dp]
@@ -194,6 +198,8 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_sample_wavelength.argtypes = [vp, C.POINTER(Request), i32, sz, dp, dp, up, dp, dp]
     L.htrdr_gpu_draw_maps_batched.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(Stats)]
     L.htrdr_gpu_draw_maps_batched_device.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(Stats)]
+    L.htrdr_gpu_draw_maps_batched_accum_device.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning),
+                                                           C.POINTER(Stats)]
     L.htrdr_gpu_autotune.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(C.c_double)]
     L.htrdr_gpu_batch_create.argtypes = [C.POINTER(BatchItem), sz, C.POINTER(Tuning), C.POINTER(C.c_void_p)]
     L.htrdr_gpu_batch_run.argtypes = [vp, C.POINTER(Stats)]
@@ -256,6 +262,12 @@ def layout_for(req: S.Request) -> BufferLayout:
     lay.elmt_size = dt.itemsize
     lay.alignment = 16
     return lay
+
+
+def accum_records(req: S.Request) -> int:
+    """Accumulator records of a map (htrdr_gpu_draw_map_accum_device): one
+    per pixel and channel, then one per pixel for the time per realisation."""
+    return req.width * req.height * ((3 if req.mode == S.MODE_IMAGE_CIE else 1) + 1)
 
 
 def props_for_mode(mode: int) -> int:
@@ -370,6 +382,23 @@ class GpuScene:
         _check(lib().htrdr_gpu_draw_map(self.handle, C.byref(r), C.byref(lay), _ptr(buf), C.byref(st)),
                "htrdr_gpu_draw_map")
         return buf, st.as_dict()
+
+    def draw_map_accum(self, req: S.Request, device_accum: int) -> dict:
+        """The map's FP64 accumulators into device memory (accum_records(req)
+        records of 32 bytes at `device_accum'); returns the stats."""
+        r = to_request(req)
+        st = Stats()
+        _check(lib().htrdr_gpu_draw_map_accum_device(self.handle, C.byref(r), C.c_void_p(device_accum),
+                                                     C.byref(st)), "htrdr_gpu_draw_map_accum_device")
+        return st.as_dict()
+
+    def finalize(self, req: S.Request, device_accum: int, device_out: int) -> None:
+        """Pixel structs of the map (device memory) from its accumulators."""
+        r = to_request(req)
+        lay = layout_for(req)
+        _check(lib().htrdr_gpu_finalize_device(self.handle, C.byref(r), C.c_void_p(device_accum),
+                                               C.byref(lay), C.c_void_p(device_out)),
+               "htrdr_gpu_finalize_device")
 
     def ground_trace(self, rays: np.ndarray, tmax: np.ndarray, from_prim: np.ndarray,
                      from_edge: np.ndarray):

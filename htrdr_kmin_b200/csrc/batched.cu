@@ -230,12 +230,15 @@ struct Plan {
   std::vector<size_t> out_off;
   DevBuf d_scenes, d_reqs, d_items, d_offsets, d_acc, d_cnt, d_out;
   size_t acc_bytes = 0;
+  bool accum_out = false; /* the items' buffers receive the accumulators */
+  std::vector<size_t> item_acc_bytes;
   PTables T{};
   WaveBufs wave; /* path slots of the wavefront engine */
 };
 
 static htrdr_gpu_res_T
-plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
+plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out,
+           bool accum_out = false)
 {
   const int device = items[0].scene ? items[0].scene->device : -1;
   for(size_t i = 0; i < n; ++i) {
@@ -243,8 +246,10 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
       return HTRDR_GPU_RES_BAD_ARG;
     const htrdr_gpu_buffer_layout& L = items[i].layout;
     const htrdr_gpu_request& q = items[i].req;
-    if(check_layout(&q, &L) != HTRDR_GPU_RES_OK) return HTRDR_GPU_RES_BAD_ARG;
+    if(!accum_out && check_layout(&q, &L) != HTRDR_GPU_RES_OK) return HTRDR_GPU_RES_BAD_ARG;
+    if(accum_out && (q.mode < 0 || q.mode > 4 || !q.width || !q.height)) return HTRDR_GPU_RES_BAD_ARG;
   }
+  P.accum_out = accum_out;
   if(!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
   P.device = device;
   P.reqs.resize(n);
@@ -276,14 +281,16 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out)
     P.out_off[i] = out_bytes;
     if(host_out) out_bytes += (items[i].layout.pitch * items[i].layout.height + 255) & ~(size_t)255;
   }
-  P.acc_bytes = acc_total * sizeof(DAccum);
-  if(!P.d_acc.alloc(P.acc_bytes) || !P.d_cnt.alloc(128) || !P.d_out.alloc(out_bytes))
+  P.acc_bytes = accum_out ? 0 : acc_total * sizeof(DAccum);
+  if((!accum_out && !P.d_acc.alloc(P.acc_bytes)) || !P.d_cnt.alloc(128) || !P.d_out.alloc(out_bytes))
     return HTRDR_GPU_RES_MEM_ERR;
+  P.item_acc_bytes.assign(n, 0);
   for(size_t i = 0; i < n; ++i) {
     const uint64_t npix = (uint64_t)P.reqs[i].width * P.reqs[i].height;
     const uint32_t nch = P.reqs[i].mode == HG_IMAGE_CIE ? 3u : 1u;
-    P.reqs[i].acc = (DAccum*)P.d_acc.ptr + acc_off[i];
+    P.reqs[i].acc = accum_out ? (DAccum*)items[i].buffer : (DAccum*)P.d_acc.ptr + acc_off[i];
     P.reqs[i].tacc = P.reqs[i].acc + npix * nch;
+    P.item_acc_bytes[i] = npix * (nch + 1) * sizeof(DAccum);
   }
   if(!P.d_scenes.upload(P.scenes.data(), P.scenes.size() * sizeof(DScene))
   || !P.d_reqs.upload(P.reqs.data(), n * sizeof(DRequest))
@@ -311,8 +318,11 @@ static bool
 plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning& tun,
              bool host_out, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1, bool capturing = false)
 {
-  bool ok = cuda_ok(cudaMemsetAsync(P.d_acc.ptr, 0, P.acc_bytes, st), "memset")
-         && cuda_ok(cudaMemsetAsync(P.d_cnt.ptr, 0, 128, st), "memset");
+  bool ok = cuda_ok(cudaMemsetAsync(P.d_cnt.ptr, 0, 128, st), "memset");
+  if(!P.accum_out)
+    ok = ok && cuda_ok(cudaMemsetAsync(P.d_acc.ptr, 0, P.acc_bytes, st), "memset");
+  for(size_t i = 0; ok && P.accum_out && i < n; ++i)
+    ok = cuda_ok(cudaMemsetAsync(P.reqs[i].acc, 0, P.item_acc_bytes[i], st), "memset");
   /* inside a stream capture an event record must be an external node to time
    * the replays */
   const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
@@ -320,7 +330,7 @@ plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_g
   if(ok) ok = cuda_ok(launch_workqueue(P.T, tun, &P.wave, P.device, st),
                       tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   if(ok && k1) ok = cuda_ok(cudaEventRecordWithFlags(k1, st, evf), "event");
-  for(size_t i = 0; ok && i < n; ++i) {
+  for(size_t i = 0; ok && !P.accum_out && i < n; ++i) {
     char* dout = host_out ? (char*)P.d_out.ptr + P.out_off[i] : (char*)items[i].buffer;
     ok = cuda_ok(launch_finalize(P.reqs[i], P.reqs[i].acc, P.reqs[i].tacc, dout,
                                  items[i].layout.pitch, st), "k_finalize");
@@ -405,14 +415,14 @@ items_tuning(const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning
 
 static htrdr_gpu_res_T
 batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuning,
-             htrdr_gpu_stats* stats, bool host)
+             htrdr_gpu_stats* stats, bool host, bool accum = false)
 {
   if(!items || !n) return HTRDR_GPU_RES_BAD_ARG;
   const htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
   if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
   take_launches();
   Plan P;
-  htrdr_gpu_res_T res = plan_build(P, items, n, host);
+  htrdr_gpu_res_T res = plan_build(P, items, n, host, accum);
   if(res != HTRDR_GPU_RES_OK) return res;
   cudaStream_t st = items[0].scene->stream;
   cudaEvent_t e0, e1, e2, e3;
@@ -448,6 +458,14 @@ try {
   return batched_impl(items, n, tuning, stats, false);
 }
 HG_API_CATCH("htrdr_gpu_draw_maps_batched_device")
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_maps_batched_accum_device(htrdr_gpu_batch_item* items, size_t n,
+                                         const htrdr_gpu_tuning* tuning, htrdr_gpu_stats* stats)
+try {
+  return batched_impl(items, n, tuning, stats, false, true);
+}
+HG_API_CATCH("htrdr_gpu_draw_maps_batched_accum_device")
 
 /* Autotuner: times every candidate -- persistent megakernel (block size x
  * queue chunk x regroup period) and wavefront (tail threshold x regroup

@@ -32,14 +32,20 @@ ensure(DevBuf& b, size_t bytes)
   return b.alloc(bytes);
 }
 
+/* One map on the scene's engine.  `user_acc' (device memory) set: the FP64
+ * accumulators are left there and no pixel struct is written (`layout' and
+ * `buffer' unused); else they live in the scene's workspace and the map is
+ * finalized into `buffer' (host or device memory). */
 htrdr_gpu_res_T
 draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
               const htrdr_gpu_buffer_layout* layout, void* buffer, bool host,
-              htrdr_gpu_stats* stats)
+              htrdr_gpu_stats* stats, DAccum* user_acc = nullptr)
 {
-  if(!scn || !buffer) return HTRDR_GPU_RES_BAD_ARG;
-  htrdr_gpu_res_T res = check_layout(req, layout);
+  if(!scn || (!buffer && !user_acc)) return HTRDR_GPU_RES_BAD_ARG;
+  htrdr_gpu_res_T res = user_acc ? HTRDR_GPU_RES_OK : check_layout(req, layout);
   if(res != HTRDR_GPU_RES_OK) return res;
+  if(user_acc && (!req || req->mode < 0 || req->mode > 4 || !req->width || !req->height))
+    return HTRDR_GPU_RES_BAD_ARG;
   if(!cuda_ok(cudaSetDevice(scn->device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
   DRequest R;
   res = make_drequest(scn, req, &R);
@@ -48,13 +54,13 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   const uint32_t npix = req->width * req->height;
   const uint32_t nch = req->mode == HG_IMAGE_CIE ? 3u : 1u;
   const size_t acc_bytes = (size_t)npix * (nch + 1) * sizeof(DAccum);
-  const size_t out_bytes = layout->pitch * layout->height;
+  const size_t out_bytes = user_acc ? 0 : layout->pitch * layout->height;
   Workspace& ws = workspace(scn);
   const bool plain = scn->engine_set && scn->engine == HTRDR_GPU_ENGINE_PLAIN;
-  if(!ensure(ws.acc, acc_bytes) || !ensure(ws.cnt, 128)) return HTRDR_GPU_RES_MEM_ERR;
+  if((!user_acc && !ensure(ws.acc, acc_bytes)) || !ensure(ws.cnt, 128)) return HTRDR_GPU_RES_MEM_ERR;
   if(!plain && !ensure(ws.tables, single_tables_bytes())) return HTRDR_GPU_RES_MEM_ERR;
   if(host && !ensure(ws.out, out_bytes)) return HTRDR_GPU_RES_MEM_ERR;
-  DAccum* acc = (DAccum*)ws.acc.ptr;
+  DAccum* acc = user_acc ? user_acc : (DAccum*)ws.acc.ptr;
   DAccum* tacc = acc + (size_t)npix * nch;
   void* dout = host ? ws.out.ptr : buffer;
   htrdr_gpu_tuning tun;
@@ -79,7 +85,8 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
                        tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   }
   cudaEventRecord(e2, st);
-  ok = ok && cuda_ok(launch_finalize(R, acc, tacc, dout, layout->pitch, st), "k_finalize");
+  if(!user_acc)
+    ok = ok && cuda_ok(launch_finalize(R, acc, tacc, dout, layout->pitch, st), "k_finalize");
   if(ok && host)
     ok = cuda_ok(cudaMemcpyAsync(buffer, dout, out_bytes, cudaMemcpyDeviceToHost, st), "D2H");
   cudaEventRecord(e3, st);
@@ -147,6 +154,37 @@ try {
   return draw_map_impl(scn, req, layout, device_buffer, false, stats);
 }
 HG_API_CATCH("htrdr_gpu_draw_map_device")
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_map_accum_device(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
+                                void* device_accum, htrdr_gpu_stats* stats)
+try {
+  if(!device_accum) return HTRDR_GPU_RES_BAD_ARG;
+  return draw_map_impl(scn, req, nullptr, nullptr, false, stats, (DAccum*)device_accum);
+}
+HG_API_CATCH("htrdr_gpu_draw_map_accum_device")
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_finalize_device(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
+                          const void* device_accum, const htrdr_gpu_buffer_layout* layout,
+                          void* device_buffer)
+try {
+  if(!scn || !device_accum || !device_buffer) return HTRDR_GPU_RES_BAD_ARG;
+  htrdr_gpu_res_T res = check_layout(req, layout);
+  if(res != HTRDR_GPU_RES_OK) return res;
+  if(!cuda_ok(cudaSetDevice(scn->device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
+  DRequest R;
+  res = make_drequest(scn, req, &R);
+  if(res != HTRDR_GPU_RES_OK) return res;
+  const uint32_t nch = req->mode == HG_IMAGE_CIE ? 3u : 1u;
+  const DAccum* acc = (const DAccum*)device_accum;
+  const DAccum* tacc = acc + (size_t)req->width * req->height * nch;
+  cudaStream_t st = scn->stream;
+  const bool ok = cuda_ok(launch_finalize(R, acc, tacc, device_buffer, layout->pitch, st), "k_finalize")
+               && cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  return ok ? HTRDR_GPU_RES_OK : HTRDR_GPU_RES_UNKNOWN_ERR;
+}
+HG_API_CATCH("htrdr_gpu_finalize_device")
 
 static htrdr_gpu_res_T
 radiance_impl(htrdr_gpu_scene* scn, int lw, size_t n, const double* pos, const double* dir,

@@ -207,6 +207,29 @@ htrdr_gpu_draw_map_device(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_
                           const struct htrdr_gpu_buffer_layout* layout, void* device_buffer,
                           struct htrdr_gpu_stats* stats);
 
+/* The map's FP64 accumulators instead of its pixel structs, for callers that
+ * combine maps drawn by several processes or GPUs and finalize once: the
+ * reference gathers the tiles of its MPI ranks into one buffer
+ * (src/core/htrdr_draw_map.c:186-268); here every rank draws the whole map on
+ * its own streams, the accumulators are summed, and htrdr_gpu_finalize_device
+ * turns the sum into pixel structs.  `device_accum' (device memory) receives
+ * width x height x channels records, then width x height more for the time
+ * per realisation, each {sum f64, sum of squares f64, count u64, failures
+ * u64} (htrdr_accum, src/core/htrdr_accum.h:31-36); channels = 3 for CIE
+ * images, else 1. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_map_accum_device(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                                void* device_accum, struct htrdr_gpu_stats* stats);
+/* Pixel structs of a map from its accumulators (the layout of
+ * htrdr_gpu_draw_map_accum_device): the estimates and standard errors
+ * (htrdr_accum_get_estimation, src/core/htrdr_accum.h:48-68) and, for
+ * longwave images, the brightness temperature
+ * (src/atmosphere/htrdr_atmosphere_draw_map.c:425-435). */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_finalize_device(struct htrdr_gpu_scene* scene, const struct htrdr_gpu_request* req,
+                          const void* device_accum, const struct htrdr_gpu_buffer_layout* layout,
+                          void* device_buffer);
+
 /* Same as htrdr_gpu_draw_map_device without allocating device memory, for
  * callers that cannot allocate while they render (an application that owns
  * all of HBM through its own pool, a loop that must not pay for the device
@@ -314,6 +337,14 @@ HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_draw_maps_batched_device(struct htrdr_gpu_batch_item* items, size_t n,
                                    const struct htrdr_gpu_tuning* tuning,
                                    struct htrdr_gpu_stats* stats);
+/* Same, each item's `buffer' (device memory) receiving the request's FP64
+ * accumulators in the layout of htrdr_gpu_draw_map_accum_device instead of
+ * its pixel structs (its `layout' is not used): the maps of several processes
+ * or GPUs are summed and finalized once with htrdr_gpu_finalize_device. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_draw_maps_batched_accum_device(struct htrdr_gpu_batch_item* items, size_t n,
+                                         const struct htrdr_gpu_tuning* tuning,
+                                         struct htrdr_gpu_stats* stats);
 HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
 /* Default tuning of a request mode: short LW paths want small blocks and
  * regrouping at every step, long SW/CIE walks larger blocks and sparser
