@@ -44,7 +44,7 @@ EXPORTED = [
     "htrdr_gpu_last_error", "htrdr_gpu_scene_set_engine", "htrdr_gpu_mode_tuning",
     "htrdr_gpu_write_image", "htrdr_gpu_ground_trace", "htrdr_gpu_draw_map_noalloc",
     "htrdr_gpu_draw_map_accum_device", "htrdr_gpu_finalize_device",
-    "htrdr_gpu_draw_maps_batched_accum_device",
+    "htrdr_gpu_draw_maps_batched_accum_device", "htrdr_gpu_server_request_launches",
 ]
 
 ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT = 0, 1, 2
@@ -211,6 +211,8 @@ def lib() -> C.CDLL:
     L.htrdr_gpu_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.htrdr_gpu_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(C.c_int)]
     L.htrdr_gpu_server_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    L.htrdr_gpu_server_request_launches.argtypes = [vp, C.c_uint64, C.POINTER(C.c_uint64),
+                                                    C.POINTER(C.c_uint64)]
     L.htrdr_gpu_server_release.argtypes = [vp]
     L.htrdr_gpu_server_release.restype = None
     L.htrdr_gpu_default_tuning.argtypes = [C.POINTER(Tuning)]
@@ -580,6 +582,13 @@ class Server:
         if res.value != RES_OK:
             raise HtrdrError("request", res.value)
         return self._bufs.pop(ticket)
+
+    def launches(self, ticket: int) -> tuple:
+        """(first, last) launch of the loop that carried the request."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().htrdr_gpu_server_request_launches(self.handle, ticket, C.byref(a), C.byref(b)),
+               "htrdr_gpu_server_request_launches")
+        return a.value, b.value
 
     def stats(self) -> dict:
         st = ServerStats()

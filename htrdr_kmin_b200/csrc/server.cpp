@@ -58,6 +58,10 @@ struct SReq {
   void* out_a = nullptr;
   cudaEvent_t copied = nullptr;
   bool finishing = false;
+  /* launches of the loop (rounds or wavefront chunks) that carried the
+   * request: the first with some of its realisations queued, and the last
+   * before all of them were known done (UINT64_MAX: none yet) */
+  uint64_t first_launch = UINT64_MAX, last_launch = 0;
 };
 
 /* Device resources of one round in flight */
@@ -155,7 +159,7 @@ struct htrdr_gpu_server {
   void loop_wave();
   bool wave_setup();
   bool wave_admit(SReq* r);
-  bool wave_append(const std::vector<SReq*>& act, uint64_t budget);
+  bool wave_append(const std::vector<SReq*>& act, uint64_t budget, uint64_t next_launch);
   PTables wave_tables_now();
 };
 
@@ -197,6 +201,8 @@ htrdr_gpu_server::launch_round(Slot& s, const std::vector<SReq*>& act)
     offsets.push_back(offsets.back() + counts[i]);
     s.parts.emplace_back(todo[i], counts[i]);
     todo[i]->next += counts[i];
+    todo[i]->first_launch = std::min(todo[i]->first_launch, seq); /* this round's index */
+    todo[i]->last_launch = std::max(todo[i]->last_launch, seq);
   }
   if(!ensure(s.scenes, scenes.size() * sizeof(DScene)) || !ensure(s.reqs, reqs.size() * sizeof(DRequest))
   || !ensure(s.items, items.size() * sizeof(PItem)) || !ensure(s.offsets, offsets.size() * 8)
@@ -436,7 +442,7 @@ htrdr_gpu_server::wave_admit(SReq* r)
 /* Fair share of `budget' realisations over the requests with work not yet
  * queued, then the leftovers in order; appends the items to the queue */
 bool
-htrdr_gpu_server::wave_append(const std::vector<SReq*>& act, uint64_t budget)
+htrdr_gpu_server::wave_append(const std::vector<SReq*>& act, uint64_t budget, uint64_t next_launch)
 {
   std::vector<SReq*> todo;
   for(SReq* r : act) if(r->state == 1 && r->next < r->total) todo.push_back(r);
@@ -463,6 +469,8 @@ htrdr_gpu_server::wave_append(const std::vector<SReq*>& act, uint64_t budget)
     end += counts[i];
     offs.push_back(end);
     todo[i]->next += counts[i];
+    /* the next launch is the first to take these realisations */
+    todo[i]->first_launch = std::min(todo[i]->first_launch, next_launch);
   }
   if(items.empty()) return true;
   const bool ok =
@@ -526,8 +534,9 @@ htrdr_gpu_server::loop_wave()
     for(SReq* r : active) {
       /* a read-back issued before the request was admitted holds another
        * request's count in its table slot */
-      if(r->finishing || r->state != 1 || r->k_admit > rb_k[b] || rb->ndone[r->rslot] < r->total)
-        continue;
+      if(r->finishing || r->state != 1 || r->k_admit > rb_k[b]) continue;
+      r->last_launch = std::max(r->last_launch, rb_k[b]);
+      if(rb->ndone[r->rslot] < r->total) continue;
       /* every realisation accumulated: the map, on the same stream */
       const bool fin = cuda_ok(launch_finalize(r->dreq, r->dreq.acc, r->dreq.tacc, r->out_a,
                                                r->layout.pitch, io), "k_finalize")
@@ -637,7 +646,7 @@ htrdr_gpu_server::loop_wave()
     const uint64_t queued = w_appended > dev_next ? w_appended - dev_next : 0;
     if(unqueued && queued < wave_P) {
       const uint64_t before = w_appended;
-      if(!wave_append(active, wave_P - queued)) { failed_gpu = true; continue; }
+      if(!wave_append(active, wave_P - queued, k)) { failed_gpu = true; continue; }
       if(w_appended > before) {
         if(!cuda_ok(wave_serve_revive(wave, io), "revive")) { failed_gpu = true; continue; }
         w_pool_live = true;
@@ -784,6 +793,22 @@ try {
   return HTRDR_GPU_RES_OK;
 }
 HG_API_CATCH("htrdr_gpu_server_wait")
+
+extern "C" HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_request_launches(htrdr_gpu_server* s, uint64_t ticket, uint64_t* first,
+                                  uint64_t* last)
+try {
+  if(!s || !first || !last) return HTRDR_GPU_RES_BAD_ARG;
+  std::lock_guard<std::mutex> lk(s->m);
+  auto it = s->all.find(ticket);
+  if(it == s->all.end()) return HTRDR_GPU_RES_BAD_ARG;
+  const SReq* r = it->second.get();
+  if(r->first_launch == UINT64_MAX) return HTRDR_GPU_RES_BAD_OP;
+  *first = r->first_launch;
+  *last = std::max(r->first_launch, r->last_launch);
+  return HTRDR_GPU_RES_OK;
+}
+HG_API_CATCH("htrdr_gpu_server_request_launches")
 
 extern "C" HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_stats(htrdr_gpu_server* s, struct htrdr_gpu_server_stats* st)

@@ -415,6 +415,15 @@ htrdr_gpu_server_wait(struct htrdr_gpu_server* server, uint64_t ticket, double t
                       htrdr_gpu_res_T* result);
 HTRDR_GPU_API htrdr_gpu_res_T
 htrdr_gpu_server_stats(struct htrdr_gpu_server* server, struct htrdr_gpu_server_stats* stats);
+/* Launches of the request loop (persistent rounds or wavefront chunks,
+ * numbered from 0 in launch order) that carried a request: `first', the
+ * first with some of its realisations queued, and `last', the last before
+ * all of them were known done.  Two requests whose ranges intersect had work
+ * on the device in the same launch (continuous batching).  No counterpart in
+ * the reference.  HTRDR_GPU_RES_BAD_OP: the request never reached the device. */
+HTRDR_GPU_API htrdr_gpu_res_T
+htrdr_gpu_server_request_launches(struct htrdr_gpu_server* server, uint64_t ticket,
+                                  uint64_t* first, uint64_t* last);
 /* Drains the submitted requests, then stops the scheduling thread */
 HTRDR_GPU_API void htrdr_gpu_server_release(struct htrdr_gpu_server* server);
 

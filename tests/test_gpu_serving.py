@@ -186,3 +186,30 @@ def test_server_kinds_change(gpu_lib, mix, name, slots, tail):
     srv.close()
     for (gs, r), got in zip(lw + sw + lw[:1], out1 + out2):
         _cmp(got, gs.draw_map(r)[0], r.mode)
+
+
+@pytest.mark.parametrize("name,slots,tail", ENGINES[:2])
+def test_request_admitted_mid_run_shares_launches(gpu_lib, mix, name, slots, tail):
+    """Continuous batching: a request submitted while another is on the GPU
+    gets its realisations into a launch that still carries the first one's
+    (their launch ranges intersect), and its map is the same as alone."""
+    api = gpu_lib
+    gs_a, r_a = mix[0]
+    big = S.Request(**{**r_a.__dict__, "width": 48, "height": 48, "spp": 64, "seed": 77})
+    gs_b, r_b = mix[4]
+    srv = api.Server(round_target_ms=2.0, round_realisations=4096,
+                     tuning=_tuning(api, _engine(api, name), slots, tail))
+    ta = srv.submit(gs_a, big)
+    t0 = time.perf_counter()
+    while srv.stats()["rounds"] < 2 and time.perf_counter() - t0 < 30:
+        time.sleep(0.001)  # the first request is on the device
+    tb = srv.submit(gs_b, r_b)
+    out_b = srv.wait(tb, WAIT_S)
+    srv.wait(ta, WAIT_S)
+    fa, la = srv.launches(ta)
+    fb, lb = srv.launches(tb)
+    srv.close()
+    print(f"{name}: first request launches {fa}..{la}, second {fb}..{lb}")
+    assert fb > fa, "the second request reached the device after the first"
+    assert fb <= la, "and shared a launch with it"
+    _cmp(out_b, gs_b.draw_map(r_b)[0], r_b.mode)
