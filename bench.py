@@ -78,7 +78,7 @@ def parse():
     p.add_argument("--rates", default="", help="serve: comma-separated arrival rates (requests/s)")
     p.add_argument("--tuning", default="",
                    help="block,chunk,period[,engine[,budget[,slots[,tail]]]] instead of the autotuner "
-                        "(engine 0 persistent, 2 wavefront)")
+                        "(engine 0 persistent, 2 wavefront, 3 sorted)")
     p.add_argument("--cpu-sample-s", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -101,7 +101,7 @@ def parse_tuning(api, text: str):
 
 
 def tuning_dict(t, source: str) -> dict:
-    d = {"engine": {0: "persistent", 2: "wavefront"}.get(t.engine, str(t.engine)),
+    d = {"engine": {0: "persistent", 2: "wavefront", 3: "sorted"}.get(t.engine, str(t.engine)),
          "block_size": t.block_size}
     if t.engine == 2:
         d.update(trace_budget=t.trace_budget or 256, wave_slots=t.wave_slots or "auto",
@@ -763,7 +763,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     alg_bytes = 16 * last.nodes + 8 * last.collisions + 32 * last.realisations
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kms * 1e-3) / 1e9
-    kernel = "wavefront" if wave else "k_persistent"
+    kernel = "wavefront" if wave else ("k_sorted" if tuning.engine == api.ENGINE_SORTED else "k_persistent")
     traffic, traffic_src = traffic_per_launch(kernel, alg_bytes)
     out_bytes = sum(d.numel() for d in su.dev)
     line = {
@@ -783,7 +783,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                      "peak_kind": peak_kind,
-                     "kernel": "k_wave_event + k_wave_trace + k_wave_finish" if wave else "k_persistent",
+                     "kernel": "k_wave_event + k_wave_trace + k_wave_finish" if wave else kernel,
                      "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": kms},
         "plain_gpu": {"value": reals / (plain_ms * 1e-3) / 1e6, "unit": UNIT, "kernel": "k_plain",
                       "kernel_ms": plain_ms, "launches": n},

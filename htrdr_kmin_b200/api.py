@@ -47,7 +47,7 @@ EXPORTED = [
     "htrdr_gpu_draw_maps_batched_accum_device", "htrdr_gpu_server_request_launches",
 ]
 
-ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT = 0, 1, 2
+ENGINE_PERSISTENT, ENGINE_PLAIN, ENGINE_WAVEFRONT, ENGINE_SORTED = 0, 1, 2, 3
 
 
 class HtrdrError(RuntimeError):

@@ -112,6 +112,118 @@ k_persistent(PTables T, int tables_in_smem)
   }
 }
 
+/* Shared-memory bytes of the sorted kernel's stage lists (two lists of slot
+ * indices and their counters) */
+__host__ __device__ constexpr size_t
+sorted_lists_bytes(uint32_t threads)
+{
+  return ((size_t)2 * threads * sizeof(uint32_t) + 4 * sizeof(uint32_t) + 15) & ~(size_t)15;
+}
+
+/* The block-sorted persistent loop.  The block's paths live in shared-memory
+ * slots that any lane may run, so every step the block sorts its slots by
+ * stage -- tracing, or waiting for an event (or for new work) -- into two
+ * lists, and lanes 0..n-1 take the n entries of each list in turn.  The
+ * warps of each pass are therefore full of lanes in the same stage (the
+ * ballot regrouping of persistent_loop only gathers the lanes a warp owns),
+ * and warps past the end of a list skip it.  `regroup_period' voxel steps are
+ * taken per trace visit.  Same state machine, same streams, same weights. */
+template <unsigned V>
+__device__ __forceinline__ void
+sorted_loop(PTables& T, PathSlot* slots, uint32_t* lists)
+{
+  const uint32_t B = blockDim.x, tid = threadIdx.x, lane = tid & 31u;
+  uint32_t* trace_list = lists;
+  uint32_t* event_list = lists + B;
+  uint32_t* n = lists + 2 * B; /* [0] tracing, [1] events, [2] queue drained */
+  unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
+  const uint32_t period = T.regroup_period > 1 ? T.regroup_period : 1;
+  {
+    Path& own = slots[tid].p;
+    own.state = ST_IDLE;
+    own.flags = 0;
+    own.c_seg = own.c_node = own.c_tc = 0;
+    own.ri = own.si = 0;
+  }
+  if(tid == 0) n[2] = 0;
+  for(;;) {
+    if(tid == 0) { n[0] = 0; n[1] = 0; }
+    __syncthreads();
+    { /* sort: each thread files the slot of its own index */
+      const uint8_t st = slots[tid].p.state;
+      const bool tr = st == ST_TRACE;
+      const bool ev = !tr && (st != ST_IDLE || !n[2]);
+      const unsigned mt = __ballot_sync(0xffffffffu, tr);
+      const unsigned me = __ballot_sync(0xffffffffu, ev);
+      uint32_t bt = 0, be = 0;
+      if(lane == 0) {
+        if(mt) bt = atomicAdd(&n[0], (uint32_t)__popc(mt));
+        if(me) be = atomicAdd(&n[1], (uint32_t)__popc(me));
+      }
+      bt = __shfl_sync(0xffffffffu, bt, 0);
+      be = __shfl_sync(0xffffffffu, be, 0);
+      const unsigned below = (1u << lane) - 1u;
+      if(tr) trace_list[bt + __popc(mt & below)] = tid;
+      if(ev) event_list[be + __popc(me & below)] = tid;
+    }
+    __syncthreads();
+    const uint32_t ntr = n[0], nev = n[1];
+    if(ntr == 0 && nev == 0) break;
+    /* trace pass */
+    if(tid < ntr) {
+      Path& p = slots[trace_list[tid]].p;
+      const DScene& S = T.scenes[p.si];
+      for(uint32_t k = 0; k < period && p.state == ST_TRACE; ++k) trace_step<V>(p, S);
+    }
+    /* event pass: accumulate finished paths, give idle slots new work, run
+     * events until the path needs a trace or ends */
+    if((tid & ~31u) < nev) { /* warps with at least one entry; all their lanes vote */
+      const bool act = tid < nev;
+      Path& p = slots[act ? event_list[tid] : 0].p;
+      if(act && p.state == ST_DONE) {
+        accumulate_b(p, T.reqs[p.ri]);
+        real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
+        fail += (p.flags & PF_FAILED) ? 1 : 0;
+        seg += p.c_seg; node += p.c_node; tc += p.c_tc;
+        p.c_seg = p.c_node = p.c_tc = 0;
+        p.state = ST_IDLE;
+      }
+      const bool need = act && p.state == ST_IDLE;
+      const unsigned m = __ballot_sync(0xffffffffu, need);
+      if(m) {
+        const unsigned leader = __ffs(m) - 1;
+        unsigned long long base = 0;
+        if(lane == leader) base = atomicAdd(T.next, (unsigned long long)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if(need) {
+          const unsigned long long g = base + (unsigned long long)__popc(m & ((1u << lane) - 1u));
+          if(g < T.total) path_assign(p, T, g);
+          else n[2] = 1; /* the queue is drained: idle slots stop asking */
+        }
+      }
+      if(act && p.state != ST_IDLE && p.state != ST_TRACE && p.state != ST_DONE) {
+        path_event<V>(p, T.scenes[p.si], T.reqs[p.ri]);
+        seg += p.c_seg; node += p.c_node; tc += p.c_tc;
+        p.c_seg = p.c_node = p.c_tc = 0;
+      }
+    }
+    __syncthreads();
+  }
+  flush_counts(T.cnt, seg, node, tc, real, fail);
+}
+
+template <unsigned V>
+__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
+k_sorted(PTables T, int tables_in_smem)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  PathSlot* slots = (PathSlot*)smem;
+  uint32_t* lists = (uint32_t*)(smem + path_slots_bytes(blockDim.x));
+  if(tables_in_smem)
+    tables_to_smem(T, smem + path_slots_bytes(blockDim.x) + sorted_lists_bytes(blockDim.x));
+  sorted_loop<V>(T, slots, lists);
+}
+
 using PersistentFn = void (*)(PTables, int);
 static PersistentFn
 persistent_fn(uint32_t v)
@@ -119,24 +231,33 @@ persistent_fn(uint32_t v)
   HG_PICK_VARIANT(v, k_persistent)
 }
 
+static PersistentFn
+sorted_fn(uint32_t v)
+{
+  HG_PICK_VARIANT(v, k_sorted)
+}
+
 bool
 valid_tuning(const htrdr_gpu_tuning& t)
 {
   return t.block_size && t.block_size <= 512 && !(t.block_size & 31) && t.queue_chunk
-      && (t.engine == HTRDR_GPU_ENGINE_PERSISTENT || t.engine == HTRDR_GPU_ENGINE_WAVEFRONT);
+      && (t.engine == HTRDR_GPU_ENGINE_PERSISTENT || t.engine == HTRDR_GPU_ENGINE_WAVEFRONT
+          || t.engine == HTRDR_GPU_ENGINE_SORTED);
 }
 
 cudaError_t
 launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm, int device,
-                  cudaStream_t st)
+                  cudaStream_t st, bool sorted)
 {
   static_assert(sizeof(DScene) % 4 == 0 && sizeof(DRequest) % 4 == 0, "word copies");
   if(!T.total) return cudaSuccess;
   const size_t tables = ((T.nscenes * sizeof(DScene) + 15) & ~(size_t)15) + T.nreqs * sizeof(DRequest);
   const int in_smem = tables <= 96 * 1024;
   const uint32_t v = hv_make((T.variant & HV_MESH) != 0, T.variant);
-  const size_t smem = (in_smem ? tables : 0) + (persistent_smem_paths(v) ? path_slots_bytes(block_size) : 0);
-  auto kern = persistent_fn(v);
+  const size_t paths = sorted ? path_slots_bytes(block_size) + sorted_lists_bytes(block_size)
+                              : (persistent_smem_paths(v) ? path_slots_bytes(block_size) : 0);
+  const size_t smem = (in_smem ? tables : 0) + paths;
+  auto kern = sorted ? sorted_fn(v) : persistent_fn(v);
   if(smem > 227 * 1024) return cudaErrorInvalidConfiguration; /* block too large for its paths */
   if(smem > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -177,7 +298,8 @@ launch_workqueue(const PTables& T0, const htrdr_gpu_tuning& tun, WaveBufs* wave,
     if(!wave) return cudaErrorInvalidValue;
     return launch_wavefront(T, tun, *wave, device, st);
   }
-  return launch_persistent(T, tun.block_size, tun.blocks_per_sm, device, st);
+  return launch_persistent(T, tun.block_size, tun.blocks_per_sm, device, st,
+                           tun.engine == HTRDR_GPU_ENGINE_SORTED);
 }
 
 cudaError_t
@@ -468,7 +590,8 @@ try {
 HG_API_CATCH("htrdr_gpu_draw_maps_batched_accum_device")
 
 /* Autotuner: times every candidate -- persistent megakernel (block size x
- * queue chunk x regroup period) and wavefront (tail threshold x regroup
+ * queue chunk x regroup period), block-sorted persistent kernel (block size x
+ * voxel steps per trace visit) and wavefront (tail threshold x regroup
  * period of its finishing megakernel) -- on the given items (device buffers)
  * with CUDA events and returns the fastest.  Results do not depend on the
  * tuning. */
@@ -500,6 +623,18 @@ try {
         t.regroup_period = p;
         if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
       }
+  }
+  static const uint32_t sblocks[] = {64, 128, 256};
+  static const uint32_t speriods[] = {1, 4};
+  htrdr_gpu_default_tuning(&t);
+  t.engine = HTRDR_GPU_ENGINE_SORTED;
+  t.queue_chunk = 1;
+  for(uint32_t b : sblocks) { /* block-sorted persistent kernel */
+    for(uint32_t p : speriods) {
+      t.block_size = b;
+      t.regroup_period = p;
+      if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
+    }
   }
   htrdr_gpu_default_tuning(&t);
   t.engine = HTRDR_GPU_ENGINE_WAVEFRONT;
@@ -555,8 +690,8 @@ try {
   htrdr_gpu_tuning tun = items_tuning(items, n, tuning);
   if(!tuning) tun.engine = HTRDR_GPU_ENGINE_PERSISTENT; /* a mode default may name the wavefront */
   if(!valid_tuning(tun)) return HTRDR_GPU_RES_BAD_ARG;
-  if(tun.engine != HTRDR_GPU_ENGINE_PERSISTENT) {
-    set_error("graph batches run the persistent engine (the wavefront's iteration count is "
+  if(tun.engine != HTRDR_GPU_ENGINE_PERSISTENT && tun.engine != HTRDR_GPU_ENGINE_SORTED) {
+    set_error("graph batches run the persistent engines (the wavefront's iteration count is "
               "decided on the host)");
     return HTRDR_GPU_RES_BAD_ARG;
   }

@@ -123,7 +123,7 @@ htrdr_gpu_scene_set_engine(htrdr_gpu_scene* scn, int engine, const htrdr_gpu_tun
 try {
   if(!scn) return HTRDR_GPU_RES_BAD_ARG;
   if(engine != HTRDR_GPU_ENGINE_PERSISTENT && engine != HTRDR_GPU_ENGINE_PLAIN
-  && engine != HTRDR_GPU_ENGINE_WAVEFRONT)
+  && engine != HTRDR_GPU_ENGINE_WAVEFRONT && engine != HTRDR_GPU_ENGINE_SORTED)
     return HTRDR_GPU_RES_BAD_ARG;
   if(tuning) {
     htrdr_gpu_tuning t = *tuning;

@@ -185,7 +185,7 @@ tables_variant(const std::vector<DScene>& scenes, const std::vector<DRequest>& r
   return hv_make(mesh, kinds);
 }
 cudaError_t launch_persistent(const PTables& T, uint32_t block_size, uint32_t blocks_per_sm,
-                              int device, cudaStream_t st);
+                              int device, cudaStream_t st, bool sorted = false);
 bool valid_tuning(const htrdr_gpu_tuning& t);
 uint64_t persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device);
 /* One request on the persistent engine.  `tables' (device memory of

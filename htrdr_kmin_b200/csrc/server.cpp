@@ -232,7 +232,8 @@ htrdr_gpu_server::launch_round(Slot& s, const std::vector<SReq*>& act)
   T.chunk = cfg.tuning.queue_chunk;
   T.regroup_period = cfg.tuning.regroup_period;
   ok = ok && cuda_ok(cudaEventRecord(s.e0, s.st), "event")
-          && cuda_ok(launch_persistent(T, cfg.tuning.block_size, cfg.tuning.blocks_per_sm, cfg.device, s.st),
+          && cuda_ok(launch_persistent(T, cfg.tuning.block_size, cfg.tuning.blocks_per_sm, cfg.device, s.st,
+                                       cfg.tuning.engine == HTRDR_GPU_ENGINE_SORTED),
                      "k_persistent")
           && cuda_ok(cudaEventRecord(s.e1, s.st), "event");
   realisations += T.total;

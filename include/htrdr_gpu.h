@@ -187,7 +187,10 @@ HTRDR_GPU_API uint32_t htrdr_gpu_scene_tree_depth(const struct htrdr_gpu_scene* 
 enum htrdr_gpu_engine {
   HTRDR_GPU_ENGINE_PERSISTENT = 0,
   HTRDR_GPU_ENGINE_PLAIN = 1,
-  HTRDR_GPU_ENGINE_WAVEFRONT = 2
+  HTRDR_GPU_ENGINE_WAVEFRONT = 2,
+  /* the persistent kernel with its paths in shared memory, regrouped by
+   * stage across the whole block at every step */
+  HTRDR_GPU_ENGINE_SORTED = 3
 };
 struct htrdr_gpu_tuning;
 /* Engine of the scene's htrdr_gpu_draw_map(_device) calls.  `tuning' (NULL:
@@ -320,7 +323,7 @@ struct htrdr_gpu_tuning {
                            * new realisations run together; 0 or 1: every step) (persistent, and
                            * the megakernel that finishes a wavefront run) */
   uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
-  uint32_t engine;        /* HTRDR_GPU_ENGINE_PERSISTENT or HTRDR_GPU_ENGINE_WAVEFRONT */
+  uint32_t engine;        /* HTRDR_GPU_ENGINE_PERSISTENT, _WAVEFRONT or _SORTED */
   uint32_t wave_slots;    /* wavefront: paths in flight (0: 2^20, at most the realisations) */
   uint32_t trace_budget;  /* wavefront: voxel steps of a trace per trace-stage visit (0: 256) */
   uint32_t wave_tail;     /* wavefront: live paths below which the remaining ones finish in one

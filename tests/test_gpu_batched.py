@@ -179,3 +179,21 @@ def test_edge_cases(gpu_lib):
                    cam_pos=(0, 0, 500), cam_tgt=(0, 1000, 500), cam_up=(0, 0, 1))
     buf, st = gsl.draw_map(r3)
     assert np.all(np.isfinite(buf["L"])) and st["failures"] == 0
+
+
+@pytest.mark.parametrize("bs,period", [(32, 1), (64, 4), (128, 1), (256, 16)])
+def test_sorted_engine_equals_plain(gpu_lib, bs, period):
+    """The block-sorted persistent kernel (paths in shared memory regrouped by
+    stage over the whole block) on a mix of SW, LW and CIE requests and on an
+    LW-only pair (its LW-only variant): the plain kernel's sums."""
+    items = _mix(gpu_lib)
+    t = gpu_lib.default_tuning()
+    t.engine, t.block_size, t.regroup_period, t.queue_chunk = gpu_lib.ENGINE_SORTED, bs, period, 1
+    for group in (items, [items[1], items[3]]):
+        bufs, st = gpu_lib.draw_maps_batched(group, t)
+        assert st["failures"] == 0
+        for (gs, req), b in zip(group, bufs):
+            gs.set_engine(gpu_lib.ENGINE_PLAIN)
+            p, _ = gs.draw_map(req)
+            gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
+            _cmp(b, p, req.mode)
