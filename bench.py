@@ -75,6 +75,8 @@ def parse():
     p.add_argument("--mix-side", default="16,96", help="mix_full: request side range (px)")
     p.add_argument("--mix-spp", default="16,128", help="mix_full: realisations per pixel range")
     p.add_argument("--no-secondary", action="store_true", help="mix_full: skip the LW flux map")
+    p.add_argument("--profile-once", action="store_true",
+                   help="one batched launch of the workload with --tuning, then its counters (for ncu)")
     p.add_argument("--rates", default="", help="serve: comma-separated arrival rates (requests/s)")
     p.add_argument("--tuning", default="",
                    help="block,chunk,period[,engine[,budget[,slots[,tail]]]] instead of the autotuner "
@@ -836,6 +838,24 @@ def main():
     for _, r in reqs:
         r.seed = M.rank_seed(r.seed, rank)  # independent streams per rank (weak scaling)
     su = Setup(api, scenes, reqs, local)
+    if args.profile_once:
+        # the launches of one step and nothing else, so that a profiler's
+        # launch list holds exactly one step
+        if not args.tuning:
+            raise SystemExit("--profile-once needs --tuning")
+        tuning = parse_tuning(api, args.tuning)
+        st = api.Stats()
+        res = api.lib().htrdr_gpu_draw_maps_batched_device(su.items_dev, su.n, C.byref(tuning), C.byref(st))
+        if res != 0:
+            raise api.HtrdrError("batched_device", res, api.lib().htrdr_gpu_last_error().decode())
+        alg = 16 * st.nodes + 8 * st.collisions + 32 * st.realisations
+        print(json.dumps({"workload": desc, "tuning": tuning_dict(tuning, "command line"),
+                          "kernel_ms": st.kernel_ms, "launches": st.launches, "alg_bytes": alg,
+                          "counters": {"segments": st.segments, "nodes": st.nodes,
+                                       "collisions": st.collisions, "realisations": st.realisations}}),
+              flush=True)
+        su.close()
+        return
     tuning, src = pick_tuning(args, api, su, args.workload)
     fields, gpu_maps, _ = measure(args, api, su, desc, tuning, src, rank, world, dist)
 

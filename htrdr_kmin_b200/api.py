@@ -24,7 +24,9 @@ import numpy as np
 from . import scene as S
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "lib", "libhtrdr_gpu.so")
+# HTRDR_GPU_LIB: another build of the library (e.g. one compiled with other
+# switches) in place of the in-tree one
+LIB_PATH = os.environ.get("HTRDR_GPU_LIB") or os.path.join(_PKG, "lib", "libhtrdr_gpu.so")
 
 RES_OK, RES_BAD_ARG, RES_MEM_ERR, RES_IO_ERR, RES_UNKNOWN_ERR, RES_BAD_OP = range(6)
 KA, KS, KEXT = 0, 1, 2

@@ -7,6 +7,22 @@
 #include "internal.h"
 #include "transport.cuh"
 
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
+/* Order of a request's realisations in the work queue: pixel-major (the
+ * realisations of a pixel are consecutive, so the lanes that take them
+ * together sample the same sensor region and often finish together) or
+ * realisation-major. */
+#ifndef HG_PIXEL_MAJOR
+#define HG_PIXEL_MAJOR 1
+#endif
+/* Lanes that finish realisations of the same pixel together add their
+ * weights with one set of atomics (cooperative-groups partition by pixel) */
+#ifndef HG_AGGREGATE
+#define HG_AGGREGATE 1
+#endif
+
 namespace {
 
 /* Item holding global realisation g: the last item whose offset is <= g */
@@ -22,7 +38,8 @@ find_item(const hg::PTables& T, uint64_t g)
 }
 
 /* Per-pixel estimator sums (src/core/htrdr_accum.h:31-68) and the
- * realisation time, for a path in ST_DONE */
+ * realisation time, for a path in ST_DONE.  Called by the lanes of a warp
+ * whose paths ended, in any subset. */
 __device__ __forceinline__ void
 accumulate_b(const Path& p, const DRequest& R)
 {
@@ -31,14 +48,38 @@ accumulate_b(const Path& p, const DRequest& R)
   const uint32_t nch = R.mode == HG_IMAGE_CIE ? 3u : 1u;
   DAccum* a = R.acc + (size_t)p.pix * nch + p.chan;
   if(p.flags & PF_FAILED) { atomicAdd(&a->pad, 1ull); return; }
+  const double us = (double)(gtimer() - p.t0) * 1e-3;
+  DAccum* t = R.tacc + p.pix;
+#if HG_AGGREGATE
+  namespace cg = cooperative_groups;
+  /* the lanes here that add to the same accumulator sum first; the time
+   * accumulator of a pixel is shared by its channels, so it is grouped by
+   * pixel apart */
+  const cg::coalesced_group here = cg::coalesced_threads();
+  const cg::coalesced_group same = cg::labeled_partition(here, (unsigned long long)(uintptr_t)a);
+  const double w = cg::reduce(same, p.weight, cg::plus<double>());
+  const double w2 = cg::reduce(same, p.weight * p.weight, cg::plus<double>());
+  if(same.thread_rank() == 0) {
+    atomicAdd(&a->s, w);
+    atomicAdd(&a->s2, w2);
+    atomicAdd(&a->n, (unsigned long long)same.size());
+  }
+  const cg::coalesced_group pix = cg::labeled_partition(here, (unsigned long long)(uintptr_t)t);
+  const double ts = cg::reduce(pix, us, cg::plus<double>());
+  const double ts2 = cg::reduce(pix, us * us, cg::plus<double>());
+  if(pix.thread_rank() == 0) {
+    atomicAdd(&t->s, ts);
+    atomicAdd(&t->s2, ts2);
+    atomicAdd(&t->n, (unsigned long long)pix.size());
+  }
+#else
   atomicAdd(&a->s, p.weight);
   atomicAdd(&a->s2, p.weight * p.weight);
   atomicAdd(&a->n, 1ull);
-  const double us = (double)(gtimer() - p.t0) * 1e-3;
-  DAccum* t = R.tacc + p.pix;
   atomicAdd(&t->s, us);
   atomicAdd(&t->s2, us * us);
   atomicAdd(&t->n, 1ull);
+#endif
 }
 
 /* Start realisation `g' (global index) in path p: request, scene, pixel and
@@ -52,9 +93,14 @@ path_assign(Path& p, const hg::PTables& T, uint64_t g)
   p.si = item.scene;
   const DRequest& R = T.reqs[item.req];
   const uint64_t local = g - __ldg(T.offsets + ii) + item.begin;
+#if HG_PIXEL_MAJOR
+  p.pix = (uint32_t)(local / R.nreal_pp);
+  p.ireal = (uint32_t)(local % R.nreal_pp);
+#else
   const uint32_t npix = R.width * R.height;
   p.ireal = (uint32_t)(local / npix);
   p.pix = (uint32_t)(local % npix);
+#endif
   p.state = ST_GEN;
 }
 
