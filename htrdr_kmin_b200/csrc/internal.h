@@ -20,6 +20,7 @@
 namespace hg {
 
 void set_error(const std::string& msg);
+const char* last_error(); /* of the calling thread */
 bool cuda_ok(cudaError_t e, const char* what);
 
 /* Handler of the function-try-block of every C entry point returning a

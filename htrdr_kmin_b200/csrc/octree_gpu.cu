@@ -20,6 +20,10 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <functional>
+#include <memory>
+#include <string>
+#include <thread>
 
 namespace hg {
 
@@ -149,9 +153,23 @@ grid_of(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
 
 }  // namespace
 
+/* Scratch and stream of one build worker: the level arrays of one tree, the
+ * depth lists of its emission and the scan's temporary storage */
+struct Worker {
+  cudaStream_t st = nullptr;
+  DevBuf kmin, kmax, leaf, lists[2], flags, rank, cubtmp;
+  size_t cub_bytes = 0;
+  std::string error;
+  ~Worker() { if(st) cudaStreamDestroy(st); }
+};
+
 /* Builds the trees of `tasks' ((quad, property) pairs) on the device into one
- * pool; tree_base/tree_count are filled per task index.  Returns false on a
- * CUDA error (message in the last error). */
+ * pool; tree_base/tree_count are filled per task index.  The trees are
+ * shared among up to 8 workers, each a host thread with its own stream and
+ * scratch (as many as fit in a quarter of the free device memory, at most
+ * 16 GB), so that the host round trips of one tree's emission overlap the
+ * others' work.  The node arrays do not depend on the number of workers.
+ * Returns false on a CUDA error (message in the last error). */
 bool
 build_octrees_gpu(const DScene& S, const float* d_lwc, const int2* d_cl, const float* d_gka,
                   const float* d_gks, const std::vector<float>& sig3, const std::vector<uint32_t>& band_of,
@@ -161,91 +179,140 @@ build_octrees_gpu(const DScene& S, const float* d_lwc, const int2* d_cl, const f
 {
   const uint32_t D = S.depth, nl = S.nlayers;
   LevelDims dims{};
-  uint64_t total_lv = 0, max_lv = 0;
+  uint64_t total_lv = 0;
   for(uint32_t L = 0; L <= D; ++L) {
     for(int a = 0; a < 3; ++a) dims.n[L][a] = (S.def[a] + (1u << L) - 1) >> L;
     dims.off[L] = total_lv;
-    const uint64_t nn = (uint64_t)dims.n[L][0] * dims.n[L][1] * dims.n[L][2];
-    total_lv += nn;
-    max_lv = std::max(max_lv, nn);
+    total_lv += (uint64_t)dims.n[L][0] * dims.n[L][1] * dims.n[L][2];
   }
   dims.off[D + 1] = total_lv;
-  DevBuf kmin, kmax, leaf, cnt, lists[2], flags, rank, cubtmp;
-  const uint64_t max_list = std::max<uint64_t>(8 * max_lv, 8);
+  /* a depth list holds the 8 children of each internal node of the depth
+   * above, whose level is >= 1: at most 8 x the size of level 1 */
+  const uint64_t n1 = D >= 1 ? (uint64_t)dims.n[1][0] * dims.n[1][1] * dims.n[1][2] : 1;
+  const uint64_t max_list = std::max<uint64_t>(8 * n1, 8);
+  const uint64_t ncell = (uint64_t)S.def[0] * S.def[1] * S.def[2];
   size_t cub_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)max_list, st);
-  if(!kmin.alloc(total_lv * 4) || !kmax.alloc(total_lv * 4) || !leaf.alloc(total_lv) || !cnt.alloc(8)
-  || !lists[0].alloc(max_list * sizeof(Entry)) || !lists[1].alloc(max_list * sizeof(Entry))
-  || !flags.alloc(max_list * 4) || !rank.alloc(max_list * 4) || !cubtmp.alloc(std::max<size_t>(cub_bytes, 16)))
-    return false;
-  const uint64_t ncell = (uint64_t)S.def[0] * S.def[1] * S.def[2];
+  cub_bytes = std::max<size_t>(cub_bytes, 16);
+  const size_t per_worker = total_lv * 9 + max_list * (2 * sizeof(Entry) + 8) + cub_bytes;
 
-  auto levels = [&](uint32_t q, int p, bool counting) -> bool {
+  int device = 0;
+  if(!cuda_ok(cudaGetDevice(&device), "cudaGetDevice") || !cuda_ok(cudaStreamSynchronize(st), "sync"))
+    return false;
+  size_t free_b = 0, total_b = 0;
+  if(!cuda_ok(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo")) return false;
+  const size_t budget = std::min<size_t>(free_b / 4, (size_t)16 << 30);
+  const size_t nw = std::max<size_t>(1, std::min<size_t>({(size_t)8, tasks.size(),
+                                                           budget / std::max<size_t>(per_worker, 1)}));
+  std::vector<std::unique_ptr<Worker>> workers;
+  for(size_t w = 0; w < nw; ++w) {
+    auto wk = std::make_unique<Worker>();
+    wk->cub_bytes = cub_bytes;
+    if(!cuda_ok(cudaStreamCreateWithFlags(&wk->st, cudaStreamNonBlocking), "stream")
+    || !wk->kmin.alloc(total_lv * 4) || !wk->kmax.alloc(total_lv * 4) || !wk->leaf.alloc(total_lv)
+    || !wk->lists[0].alloc(max_list * sizeof(Entry)) || !wk->lists[1].alloc(max_list * sizeof(Entry))
+    || !wk->flags.alloc(max_list * 4) || !wk->rank.alloc(max_list * 4) || !wk->cubtmp.alloc(cub_bytes))
+      return false;
+    workers.push_back(std::move(wk));
+  }
+  DevBuf counts;
+  if(!counts.alloc(std::max<size_t>(tasks.size(), 1) * 8)
+  || !cuda_ok(cudaMemsetAsync(counts.ptr, 0, std::max<size_t>(tasks.size(), 1) * 8, st), "memset")
+  || !cuda_ok(cudaStreamSynchronize(st), "sync"))
+    return false;
+
+  /* the levels of task t on worker w (counting: its internal nodes into counts[t]) */
+  auto levels = [&](Worker& w, size_t t, bool counting) -> bool {
+    const uint32_t q = tasks[t].first;
+    const int p = tasks[t].second;
     const float sig = sig3[band_of[q] * 3 + p];
-    k_level0<<<grid_of(ncell, 256), 256, 0, st>>>(d_lwc, S.def[0], S.def[1], S.def[2], d_cl,
-      d_gka + (size_t)q * nl, d_gks + (size_t)q * nl, sig, p, (float*)kmin.ptr, (float*)kmax.ptr,
-      (uint8_t*)leaf.ptr);
-    if(counting && cudaMemsetAsync(cnt.ptr, 0, 8, st) != cudaSuccess) return false;
+    k_level0<<<grid_of(ncell, 256), 256, 0, w.st>>>(d_lwc, S.def[0], S.def[1], S.def[2], d_cl,
+      d_gka + (size_t)q * nl, d_gks + (size_t)q * nl, sig, p, (float*)w.kmin.ptr, (float*)w.kmax.ptr,
+      (uint8_t*)w.leaf.ptr);
     for(uint32_t L = 1; L <= D; ++L) {
       const uint64_t np = (uint64_t)dims.n[L][0] * dims.n[L][1] * dims.n[L][2];
-      k_level<<<grid_of(np, 256), 256, 0, st>>>(L, dims, (float*)kmin.ptr, (float*)kmax.ptr,
-        (uint8_t*)leaf.ptr, level_force, (double)(1u << L) * cmax, tau,
-        counting ? (unsigned long long*)cnt.ptr : nullptr);
+      k_level<<<grid_of(np, 256), 256, 0, w.st>>>(L, dims, (float*)w.kmin.ptr, (float*)w.kmax.ptr,
+        (uint8_t*)w.leaf.ptr, level_force, (double)(1u << L) * cmax, tau,
+        counting ? (unsigned long long*)counts.ptr + t : nullptr);
     }
     return cuda_ok(cudaGetLastError(), "octree levels");
   };
 
-  /* pass 1: node counts */
-  base.assign(tasks.size(), 0);
-  count.assign(tasks.size(), 0);
-  uint64_t total_nodes = 0;
-  for(size_t t = 0; t < tasks.size(); ++t) {
-    if(!levels(tasks[t].first, tasks[t].second, true)) return false;
-    unsigned long long ni = 0;
-    if(!cuda_ok(cudaMemcpyAsync(&ni, cnt.ptr, 8, cudaMemcpyDeviceToHost, st), "D2H")
-    || !cuda_ok(cudaStreamSynchronize(st), "sync"))
-      return false;
-    base[t] = total_nodes;
-    count[t] = 1 + 8 * ni;
-    total_nodes += count[t];
-  }
-  if(!pool.alloc(total_nodes * 16)) return false;
-
-  /* pass 2: emission */
-  for(size_t t = 0; t < tasks.size(); ++t) {
-    if(!levels(tasks[t].first, tasks[t].second, false)) return false;
+  /* the breadth-first emission of task t into the pool */
+  auto emit = [&](Worker& w, size_t t) -> bool {
     uint4* nodes = (uint4*)pool.ptr + base[t];
     const Entry root{D, 0, 0, 0};
-    if(!cuda_ok(cudaMemcpyAsync(lists[0].ptr, &root, sizeof(Entry), cudaMemcpyHostToDevice, st), "H2D"))
+    if(!cuda_ok(cudaMemcpyAsync(w.lists[0].ptr, &root, sizeof(Entry), cudaMemcpyHostToDevice, w.st), "H2D"))
       return false;
     uint32_t cur = 0, n_d = 1, base_d = 0;
     while(n_d) {
-      k_flags<<<grid_of(n_d, 256), 256, 0, st>>>((const Entry*)lists[cur].ptr, n_d, dims,
-                                                  (const uint8_t*)leaf.ptr, (uint32_t*)flags.ptr);
-      size_t tb = cub_bytes;
-      if(cub::DeviceScan::ExclusiveSum(cubtmp.ptr, tb, (uint32_t*)flags.ptr, (uint32_t*)rank.ptr,
-                                       (int)n_d, st) != cudaSuccess)
+      k_flags<<<grid_of(n_d, 256), 256, 0, w.st>>>((const Entry*)w.lists[cur].ptr, n_d, dims,
+                                                    (const uint8_t*)w.leaf.ptr, (uint32_t*)w.flags.ptr);
+      size_t tb = w.cub_bytes;
+      if(cub::DeviceScan::ExclusiveSum(w.cubtmp.ptr, tb, (uint32_t*)w.flags.ptr, (uint32_t*)w.rank.ptr,
+                                       (int)n_d, w.st) != cudaSuccess)
         return cuda_ok(cudaGetLastError(), "scan");
-      uint32_t last_flag = 0, last_rank = 0;
-      if(!cuda_ok(cudaMemcpyAsync(&last_flag, (uint32_t*)flags.ptr + n_d - 1, 4, cudaMemcpyDeviceToHost, st), "D2H")
-      || !cuda_ok(cudaMemcpyAsync(&last_rank, (uint32_t*)rank.ptr + n_d - 1, 4, cudaMemcpyDeviceToHost, st), "D2H"))
+      uint32_t last[2] = {0, 0}; /* flag and rank of the last entry */
+      if(!cuda_ok(cudaMemcpyAsync(&last[0], (uint32_t*)w.flags.ptr + n_d - 1, 4, cudaMemcpyDeviceToHost, w.st), "D2H")
+      || !cuda_ok(cudaMemcpyAsync(&last[1], (uint32_t*)w.rank.ptr + n_d - 1, 4, cudaMemcpyDeviceToHost, w.st), "D2H"))
         return false;
       const uint32_t base_next = base_d + n_d;
-      k_emit<<<grid_of(n_d, 256), 256, 0, st>>>((const Entry*)lists[cur].ptr, n_d, dims,
-        (const float*)kmin.ptr, (const float*)kmax.ptr, (const uint32_t*)flags.ptr,
-        (const uint32_t*)rank.ptr, base_d, base_next, nodes, (Entry*)lists[cur ^ 1].ptr);
-      if(!cuda_ok(cudaStreamSynchronize(st), "sync")) return false;
-      const uint32_t n_internal = last_rank + last_flag;
+      k_emit<<<grid_of(n_d, 256), 256, 0, w.st>>>((const Entry*)w.lists[cur].ptr, n_d, dims,
+        (const float*)w.kmin.ptr, (const float*)w.kmax.ptr, (const uint32_t*)w.flags.ptr,
+        (const uint32_t*)w.rank.ptr, base_d, base_next, nodes, (Entry*)w.lists[cur ^ 1].ptr);
+      if(!cuda_ok(cudaStreamSynchronize(w.st), "sync")) return false;
+      const uint64_t n_next = 8ull * ((uint64_t)last[1] + last[0]);
+      if(n_next > max_list) { set_error("octree emission: depth list overflow"); return false; }
       base_d = base_next;
-      n_d = 8 * n_internal;
+      n_d = (uint32_t)n_next;
       cur ^= 1;
     }
     if(base_d != count[t]) {
       set_error("octree emission: node count mismatch");
       return false;
     }
+    return true;
+  };
+
+  /* run `job' on every task, task t on worker t % nw, one host thread per worker */
+  auto run = [&](const std::function<bool(Worker&, size_t)>& job) -> bool {
+    std::vector<std::thread> th;
+    std::vector<int> ok(nw, 1);
+    for(size_t w = 0; w < nw; ++w) {
+      th.emplace_back([&, w]() {
+        cudaSetDevice(device);
+        for(size_t t = w; t < tasks.size() && ok[w]; t += nw)
+          if(!job(*workers[w], t)) { ok[w] = 0; workers[w]->error = last_error(); }
+        if(ok[w] && !cuda_ok(cudaStreamSynchronize(workers[w]->st), "sync")) {
+          ok[w] = 0;
+          workers[w]->error = last_error();
+        }
+      });
+    }
+    for(auto& x : th) x.join();
+    for(size_t w = 0; w < nw; ++w)
+      if(!ok[w]) { set_error(workers[w]->error); return false; }
+    return true;
+  };
+
+  /* pass 1: node counts */
+  if(!run([&](Worker& w, size_t t) { return levels(w, t, true); })) return false;
+  std::vector<unsigned long long> ni(tasks.size(), 0);
+  if(!tasks.empty()
+  && !cuda_ok(cudaMemcpy(ni.data(), counts.ptr, tasks.size() * 8, cudaMemcpyDeviceToHost), "D2H"))
+    return false;
+  base.assign(tasks.size(), 0);
+  count.assign(tasks.size(), 0);
+  uint64_t total_nodes = 0;
+  for(size_t t = 0; t < tasks.size(); ++t) {
+    base[t] = total_nodes;
+    count[t] = 1 + 8 * ni[t];
+    total_nodes += count[t];
   }
-  return true;
+  if(!pool.alloc(total_nodes * 16)) return false;
+
+  /* pass 2: levels again, then emission */
+  return run([&](Worker& w, size_t t) { return levels(w, t, false) && emit(w, t); });
 }
 
 }  // namespace hg
