@@ -146,3 +146,22 @@ def test_golden_vectors_are_the_reference_outputs(ref_lib, name, scene, req, pro
     mq = S.Request(**{**req.__dict__, "seed": G.MAP_SEED, "spp": G.MAP_SPP[name]})
     for k, v in G.map_fields(rs.draw_map(mq), req.mode).items():
         np.testing.assert_array_equal(v, golden[f"{name}/map_{k}"])
+
+
+def _batched_cases():
+    """The request kinds of the batched workloads (8 bands x 4 points, SW and
+    LW bands in one scene, repeated power-law cloud) on a reduced scene."""
+    sc = S.batched_scenes(scale=1 / 16)[1]
+    reqs = S.batched_requests(n=2, side_range=(6, 6), spp_range=(8, 8))
+    return [("batched_sw", sc, reqs[0][1], 0b111), ("batched_lw", sc, reqs[1][1], 0b111)]
+
+
+@pytest.mark.parametrize("name,scene,req,props", _batched_cases(), ids=_ids)
+def test_batched_kinds_equal_the_reference(ref_lib, oracle_lib, name, scene, req, props):
+    npix = req.width * req.height
+    wr = ref_lib.RefScene(scene, props).realisation_weights(req, 0, npix)
+    wo = oracle_lib.OracleScene(scene, props).realisation_weights(req, 0, npix)
+    np.testing.assert_array_equal(np.isnan(wr), np.isnan(wo))
+    rel = np.abs(wo - wr) / np.maximum(np.abs(wr), 1e-300)
+    print(f"{name}: {wr.size} realisations, max rel {np.nanmax(rel):.2e}")
+    assert np.nanmax(rel) <= REL
