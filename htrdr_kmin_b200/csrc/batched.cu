@@ -112,106 +112,6 @@ k_persistent(PTables T, int tables_in_smem)
   }
 }
 
-/* Shared-memory bytes of the sorted kernel's stage lists (two lists of slot
- * indices and their counters) */
-__host__ __device__ constexpr size_t
-sorted_lists_bytes(uint32_t threads)
-{
-  return ((size_t)2 * threads * sizeof(uint32_t) + 4 * sizeof(uint32_t) + 15) & ~(size_t)15;
-}
-
-/* The block-sorted persistent loop.  The block's paths live in shared-memory
- * slots that any lane may run, so every step the block sorts its slots by
- * stage -- tracing, or waiting for an event (or for new work) -- into two
- * lists, and lanes 0..n-1 take the n entries of each list in turn.  The
- * warps of each pass are therefore full of lanes in the same stage (the
- * ballot regrouping of persistent_loop only gathers the lanes a warp owns),
- * and warps past the end of a list skip it.  `regroup_period' voxel steps are
- * taken per trace visit.  Same state machine, same streams, same weights. */
-template <unsigned V>
-__device__ __forceinline__ void
-sorted_loop(PTables& T, PathSlot* slots, uint32_t* lists)
-{
-  const uint32_t B = blockDim.x, tid = threadIdx.x, lane = tid & 31u;
-  uint32_t* trace_list = lists;
-  uint32_t* event_list = lists + B;
-  uint32_t* n = lists + 2 * B; /* [0] tracing, [1] events, [2] queue drained */
-  unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
-  const uint32_t period = T.regroup_period > 1 ? T.regroup_period : 1;
-  {
-    Path& own = slots[tid].p;
-    own.state = ST_IDLE;
-    own.flags = 0;
-    own.c_seg = own.c_node = own.c_tc = 0;
-    own.ri = own.si = 0;
-  }
-  if(tid == 0) n[2] = 0;
-  for(;;) {
-    if(tid == 0) { n[0] = 0; n[1] = 0; }
-    __syncthreads();
-    { /* sort: each thread files the slot of its own index */
-      const uint8_t st = slots[tid].p.state;
-      const bool tr = st == ST_TRACE;
-      const bool ev = !tr && (st != ST_IDLE || !n[2]);
-      const unsigned mt = __ballot_sync(0xffffffffu, tr);
-      const unsigned me = __ballot_sync(0xffffffffu, ev);
-      uint32_t bt = 0, be = 0;
-      if(lane == 0) {
-        if(mt) bt = atomicAdd(&n[0], (uint32_t)__popc(mt));
-        if(me) be = atomicAdd(&n[1], (uint32_t)__popc(me));
-      }
-      bt = __shfl_sync(0xffffffffu, bt, 0);
-      be = __shfl_sync(0xffffffffu, be, 0);
-      const unsigned below = (1u << lane) - 1u;
-      if(tr) trace_list[bt + __popc(mt & below)] = tid;
-      if(ev) event_list[be + __popc(me & below)] = tid;
-    }
-    __syncthreads();
-    const uint32_t ntr = n[0], nev = n[1];
-    if(ntr == 0 && nev == 0) break;
-    /* trace pass */
-    if(tid < ntr) {
-      Path& p = slots[trace_list[tid]].p;
-      const DScene& S = T.scenes[p.si];
-      for(uint32_t k = 0; k < period && p.state == ST_TRACE; ++k) trace_step<V>(p, S);
-    }
-    /* event pass: accumulate finished paths, give idle slots new work, run
-     * events until the path needs a trace or ends */
-    if((tid & ~31u) < nev) { /* warps with at least one entry; all their lanes vote */
-      const bool act = tid < nev;
-      Path& p = slots[act ? event_list[tid] : 0].p;
-      if(act && p.state == ST_DONE) {
-        accumulate_b(p, T.reqs[p.ri]);
-        real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
-        fail += (p.flags & PF_FAILED) ? 1 : 0;
-        seg += p.c_seg; node += p.c_node; tc += p.c_tc;
-        p.c_seg = p.c_node = p.c_tc = 0;
-        p.state = ST_IDLE;
-      }
-      const bool need = act && p.state == ST_IDLE;
-      const unsigned m = __ballot_sync(0xffffffffu, need);
-      if(m) {
-        const unsigned leader = __ffs(m) - 1;
-        unsigned long long base = 0;
-        if(lane == leader) base = atomicAdd(T.next, (unsigned long long)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if(need) {
-          const unsigned long long g = base + (unsigned long long)__popc(m & ((1u << lane) - 1u));
-          if(g < T.total) path_assign(p, T, g);
-          else n[2] = 1; /* the queue is drained: idle slots stop asking */
-        }
-      }
-      if(act && p.state != ST_IDLE && p.state != ST_TRACE && p.state != ST_DONE) {
-        path_event<V>(p, T.scenes[p.si], T.reqs[p.ri]);
-        seg += p.c_seg; node += p.c_node; tc += p.c_tc;
-        p.c_seg = p.c_node = p.c_tc = 0;
-      }
-    }
-    __syncthreads();
-  }
-  flush_counts(T.cnt, seg, node, tc, real, fail);
-}
-
 template <unsigned V>
 __global__ void __maxnreg__(HG_PERSIST_MAXNREG)
 k_sorted(PTables T, int tables_in_smem)
@@ -221,7 +121,7 @@ k_sorted(PTables T, int tables_in_smem)
   uint32_t* lists = (uint32_t*)(smem + path_slots_bytes(blockDim.x));
   if(tables_in_smem)
     tables_to_smem(T, smem + path_slots_bytes(blockDim.x) + sorted_lists_bytes(blockDim.x));
-  sorted_loop<V>(T, slots, lists);
+  sorted_loop<V>(T, slots, lists, NoResume{});
 }
 
 using PersistentFn = void (*)(PTables, int);

@@ -30,6 +30,12 @@
 #include <algorithm>
 #include <cstring>
 
+/* Tail kernel of a run: the block-sorted loop over shared-memory path slots
+ * (1) or the register-resident megakernel (0) */
+#ifndef HG_WAVE_SORTED_TAIL
+#define HG_WAVE_SORTED_TAIL 0
+#endif
+
 namespace hg {
 
 namespace {
@@ -385,6 +391,50 @@ k_wave_finish(WTables W, int tables_in_smem)
   flush_counts(T.cnt, seg, node, tc, real, fail);
 }
 
+/* Saved paths of live list 0, resumed by the sorted finishing kernel: a
+ * warp takes its idle lanes' entries with one atomic; the lane past the end
+ * of the list marks it exhausted */
+struct ResumeLive {
+  static constexpr bool kActive = true;
+  const uint4* paths;
+  const uint32_t* list0;
+  WCtl* ctl;
+  uint32_t n;
+  __device__ __forceinline__ bool
+  take(Path& p, bool want, unsigned lane, uint32_t* exhausted) const
+  {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if(!m) return false;
+    const unsigned leader = __ffs(m) - 1;
+    uint32_t i0 = 0;
+    if(lane == leader) i0 = atomicAdd(&ctl->fetch_finish, (uint32_t)__popc(m));
+    i0 = __shfl_sync(0xffffffffu, i0, leader);
+    if(!want) return false;
+    const uint32_t idx = i0 + __popc(m & ((1u << lane) - 1u));
+    if(idx >= n) { *exhausted = 1; return false; }
+    load_path(p, paths + (size_t)list0[idx] * kPathV4);
+    p.t0 = gtimer() - p.t0; /* stored: busy time so far */
+    return true;
+  }
+};
+
+/* The tail on the block-sorted loop: the saved paths of live list 0 and then
+ * the queue, run from shared-memory slots regrouped by stage over the whole
+ * block at every step */
+template <unsigned V>
+__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
+k_wave_finish_sorted(WTables W, int tables_in_smem)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  PTables T = W.T;
+  PathSlot* slots = (PathSlot*)smem;
+  uint32_t* lists = (uint32_t*)(smem + path_slots_bytes(blockDim.x));
+  if(tables_in_smem)
+    tables_to_smem(T, smem + path_slots_bytes(blockDim.x) + sorted_lists_bytes(blockDim.x));
+  const ResumeLive src{W.paths, W.list0, W.ctl, W.ctl->n_live[0]};
+  sorted_loop<V>(T, slots, lists, src);
+}
+
 size_t
 wave_slot_bytes()
 {
@@ -441,12 +491,17 @@ wave_event_fn(uint32_t v)
 WaveFinishFn
 wave_finish_fn(uint32_t v)
 {
+#if HG_WAVE_SORTED_TAIL
+  HG_PICK_VARIANT(v, k_wave_finish_sorted)
+#else
   HG_PICK_VARIANT(v, k_wave_finish)
+#endif
 }
 
 /* Launch shapes of a run over the tables T */
 struct WaveLaunch {
   size_t smem = 0;
+  size_t fi_smem = 0; /* of the finishing kernel (its path slots when sorted) */
   int in_smem = 0;
   unsigned ev_grid = 0, tr_grid = 0, fi_grid = 0;
   uint32_t tb = 256;
@@ -465,21 +520,28 @@ wave_params(const PTables& T, const htrdr_gpu_tuning& tun, int device, WaveLaunc
   L.smem = L.in_smem ? tables : 0;
   L.ev = wave_event_fn(T.variant);
   L.fi = wave_finish_fn(T.variant);
+  L.tb = tun.block_size ? tun.block_size : 256;
+#if HG_WAVE_SORTED_TAIL
+  L.fi_smem = L.smem + path_slots_bytes(L.tb) + sorted_lists_bytes(L.tb);
+  if(L.fi_smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+#else
+  L.fi_smem = L.smem;
+#endif
   cudaError_t e;
   if(L.smem > 48 * 1024) {
     if((e = cudaFuncSetAttribute(L.ev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
       return e;
     if((e = cudaFuncSetAttribute(k_wave_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
       return e;
-    if((e = cudaFuncSetAttribute(L.fi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
-      return e;
   }
+  if(L.fi_smem > 48 * 1024
+  && (e = cudaFuncSetAttribute(L.fi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.fi_smem)))
+    return e;
   int nsm = 0, ev_per_sm = 0, tr_per_sm = 0, fi_per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  L.tb = tun.block_size ? tun.block_size : 256;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ev_per_sm, L.ev, 128, L.smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, k_wave_trace, (int)L.tb, L.smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, L.fi, (int)L.tb, L.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fi_per_sm, L.fi, (int)L.tb, L.fi_smem);
   if(tun.blocks_per_sm) tr_per_sm = std::min(tr_per_sm, (int)tun.blocks_per_sm);
   L.ev_grid = (unsigned)(nsm * std::max(ev_per_sm, 1));
   L.tr_grid = (unsigned)(nsm * std::max(tr_per_sm, 1));
@@ -535,7 +597,7 @@ launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int
    * whole queue */
   if(P < L.tail) {
     k_wave_init<<<1, 32, 0, st>>>(W, 0u);
-    L.fi<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+    L.fi<<<L.fi_grid, L.tb, L.fi_smem, st>>>(W, L.in_smem);
     note_launches(2);
     return cudaGetLastError();
   }
@@ -563,7 +625,7 @@ launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, int
       const uint32_t live = hctl[(k - 1) & 1].n_live[0];
       if(live == 0) break;  /* chunk k runs empty stages */
       if(live < L.tail) {   /* after chunk k, the megakernel finishes list 0 */
-        L.fi<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+        L.fi<<<L.fi_grid, L.tb, L.fi_smem, st>>>(W, L.in_smem);
         note_launches(1);
         return cudaGetLastError();
       }
@@ -622,7 +684,7 @@ wave_serve_finish(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B, in
   cudaError_t e = wave_params(T, tun, device, L);
   if(e) return e;
   const WTables W = wave_tables(T, tun, B, true);
-  L.fi<<<L.fi_grid, L.tb, L.smem, st>>>(W, L.in_smem);
+  L.fi<<<L.fi_grid, L.tb, L.fi_smem, st>>>(W, L.in_smem);
   k_wave_clamp<<<1, 32, 0, st>>>(W);
   note_launches(2);
   if((e = cudaGetLastError())) return e;
