@@ -1,8 +1,8 @@
 """Benchmark of the B200 atmosphere path tracer (one JSON line on rank 0).
 
 Default workload (``--workload mix_full``), the batched configuration the
-metric names: 64 uneven image requests -- side log-uniform in [16, 96] px,
-16 to 128 realisations per pixel log-uniform, 50 % shortwave / 50 % longwave
+metric names: 64 uneven image requests -- side log-uniform in [16, 64] px,
+16 to 64 realisations per pixel log-uniform, 50 % shortwave / 50 % longwave
 -- each on one of three full-size seeded cloud scenes (128^3, 256x256x64 and
 512x512x128 cells of 50 m, 8 bands x 4 quadrature points, 50 gas layers);
 the request sizes are reduced from log-U[32,1024] px and [16,1024]
@@ -72,8 +72,8 @@ def parse():
     p.add_argument("--workload", default="mix_full",
                    choices=["mix_full", "lw_flux", "sw_image", "sw_large", "cie_image", "cie_full",
                             "mix", "serve"])
-    p.add_argument("--mix-side", default="16,96", help="mix_full: request side range (px)")
-    p.add_argument("--mix-spp", default="16,128", help="mix_full: realisations per pixel range")
+    p.add_argument("--mix-side", default="16,64", help="mix_full: request side range (px)")
+    p.add_argument("--mix-spp", default="16,64", help="mix_full: realisations per pixel range")
     p.add_argument("--no-secondary", action="store_true", help="mix_full: skip the LW flux map")
     p.add_argument("--profile-once", action="store_true",
                    help="one batched launch of the workload with --tuning, then its counters (for ncu)")
@@ -260,8 +260,8 @@ def _range(text: str):
 def workload(name: str, args=None):
     """Scenes, list of (scene index, request) and a description."""
     if name == "mix_full":
-        side = _range(args.mix_side) if args is not None else (16, 96)
-        spp = _range(args.mix_spp) if args is not None else (16, 128)
+        side = _range(args.mix_side) if args is not None else (16, 64)
+        spp = _range(args.mix_spp) if args is not None else (16, 64)
         scenes = S.batched_scenes(scale=1.0)
         reqs = S.batched_requests(n=64, side_range=side, spp_range=spp)
         return scenes, reqs, (

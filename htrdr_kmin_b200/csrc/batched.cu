@@ -490,8 +490,7 @@ try {
 HG_API_CATCH("htrdr_gpu_draw_maps_batched_accum_device")
 
 /* Autotuner: times every candidate -- persistent megakernel (block size x
- * queue chunk x regroup period), block-sorted persistent kernel (block size x
- * voxel steps per trace visit) and wavefront (tail threshold x regroup
+ * queue chunk x regroup period) and wavefront (tail threshold x regroup
  * period of its finishing megakernel) -- on the given items (device buffers)
  * with CUDA events and returns the fastest.  Results do not depend on the
  * tuning. */
@@ -523,18 +522,6 @@ try {
         t.regroup_period = p;
         if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
       }
-  }
-  static const uint32_t sblocks[] = {64, 128, 256};
-  static const uint32_t speriods[] = {1, 4};
-  htrdr_gpu_default_tuning(&t);
-  t.engine = HTRDR_GPU_ENGINE_SORTED;
-  t.queue_chunk = 1;
-  for(uint32_t b : sblocks) { /* block-sorted persistent kernel */
-    for(uint32_t p : speriods) {
-      t.block_size = b;
-      t.regroup_period = p;
-      if((res = time_it(t)) != HTRDR_GPU_RES_OK) return res;
-    }
   }
   htrdr_gpu_default_tuning(&t);
   t.engine = HTRDR_GPU_ENGINE_WAVEFRONT;

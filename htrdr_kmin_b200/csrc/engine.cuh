@@ -10,17 +10,20 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 
-/* Order of a request's realisations in the work queue: pixel-major (the
- * realisations of a pixel are consecutive, so the lanes that take them
- * together sample the same sensor region and often finish together) or
- * realisation-major. */
+/* Order of a request's realisations in the work queue: realisation-major
+ * (0: consecutive realisations are on different pixels) or pixel-major (1:
+ * the realisations of a pixel are consecutive, so the lanes that take them
+ * together sample the same sensor region).  Realisation-major measured
+ * faster: 121.6 against 100.2 Mrealisations/s on the LW flux map with the
+ * aggregation below, equal on the SW/LW mix. */
 #ifndef HG_PIXEL_MAJOR
-#define HG_PIXEL_MAJOR 1
+#define HG_PIXEL_MAJOR 0
 #endif
 /* Lanes that finish realisations of the same pixel together add their
- * weights with one set of atomics (cooperative-groups partition by pixel) */
+ * weights with one set of atomics (cooperative-groups partition by pixel);
+ * off by default (see above). */
 #ifndef HG_AGGREGATE
-#define HG_AGGREGATE 1
+#define HG_AGGREGATE 0
 #endif
 
 namespace {
