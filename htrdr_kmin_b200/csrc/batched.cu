@@ -121,7 +121,7 @@ k_sorted(PTables T, int tables_in_smem)
   uint32_t* lists = (uint32_t*)(smem + path_slots_bytes(blockDim.x));
   if(tables_in_smem)
     tables_to_smem(T, smem + path_slots_bytes(blockDim.x) + sorted_lists_bytes(blockDim.x));
-  sorted_loop<V>(T, slots, lists, NoResume{});
+  sorted_loop<V>(T, slots, lists);
 }
 
 using PersistentFn = void (*)(PTables, int);

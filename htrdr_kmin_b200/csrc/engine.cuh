@@ -203,13 +203,6 @@ sorted_lists_bytes(uint32_t threads)
   return ((size_t)2 * threads * sizeof(uint32_t) + 4 * sizeof(uint32_t) + 15) & ~(size_t)15;
 }
 
-/* Source of saved paths an idle slot resumes before it takes new work: none
- * for a persistent launch (the wavefront's tail resumes its live paths) */
-struct NoResume {
-  static constexpr bool kActive = false;
-  __device__ __forceinline__ bool take(Path&, bool, unsigned, uint32_t*) const { return false; }
-};
-
 /* The block-sorted loop.  The block's paths live in shared-memory
  * slots that any lane may run, so every step the block sorts its slots by
  * stage -- tracing, or waiting for an event (or for new work) -- into two
@@ -218,14 +211,14 @@ struct NoResume {
  * ballot regrouping of persistent_loop only gathers the lanes a warp owns),
  * and warps past the end of a list skip it.  `regroup_period' voxel steps are
  * taken per trace visit.  Same state machine, same streams, same weights. */
-template <unsigned V, class Resume>
+template <unsigned V>
 __device__ __forceinline__ void
-sorted_loop(hg::PTables& T, PathSlot* slots, uint32_t* lists, const Resume& resume)
+sorted_loop(hg::PTables& T, PathSlot* slots, uint32_t* lists)
 {
   const uint32_t B = blockDim.x, tid = threadIdx.x, lane = tid & 31u;
   uint32_t* trace_list = lists;
   uint32_t* event_list = lists + B;
-  uint32_t* n = lists + 2 * B; /* [0] tracing, [1] events, [2] queue drained, [3] no saved path left */
+  uint32_t* n = lists + 2 * B; /* [0] tracing, [1] events, [2] queue drained */
   unsigned long long seg = 0, node = 0, tc = 0, real = 0, fail = 0;
   const uint32_t period = T.regroup_period > 1 ? T.regroup_period : 1;
   {
@@ -235,14 +228,14 @@ sorted_loop(hg::PTables& T, PathSlot* slots, uint32_t* lists, const Resume& resu
     own.c_seg = own.c_node = own.c_tc = 0;
     own.ri = own.si = 0;
   }
-  if(tid == 0) { n[2] = 0; n[3] = Resume::kActive ? 0u : 1u; }
+  if(tid == 0) n[2] = 0;
   for(;;) {
     if(tid == 0) { n[0] = 0; n[1] = 0; }
     __syncthreads();
     { /* sort: each thread files the slot of its own index */
       const uint8_t st = slots[tid].p.state;
       const bool tr = st == ST_TRACE;
-      const bool ev = !tr && (st != ST_IDLE || !n[2] || !n[3]);
+      const bool ev = !tr && (st != ST_IDLE || !n[2]);
       const unsigned mt = __ballot_sync(0xffffffffu, tr);
       const unsigned me = __ballot_sync(0xffffffffu, ev);
       uint32_t bt = 0, be = 0;
@@ -277,10 +270,6 @@ sorted_loop(hg::PTables& T, PathSlot* slots, uint32_t* lists, const Resume& resu
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
         p.c_seg = p.c_node = p.c_tc = 0;
         p.state = ST_IDLE;
-      }
-      if constexpr(Resume::kActive) { /* saved paths first */
-        const bool want = act && p.state == ST_IDLE && !n[3];
-        resume.take(p, want, lane, &n[3]);
       }
       const bool need = act && p.state == ST_IDLE && !n[2];
       const unsigned m = __ballot_sync(0xffffffffu, need);

@@ -30,12 +30,6 @@
 #include <algorithm>
 #include <cstring>
 
-/* Tail kernel of a run: the block-sorted loop over shared-memory path slots
- * (1) or the register-resident megakernel (0) */
-#ifndef HG_WAVE_SORTED_TAIL
-#define HG_WAVE_SORTED_TAIL 0
-#endif
-
 namespace hg {
 
 namespace {
@@ -391,50 +385,6 @@ k_wave_finish(WTables W, int tables_in_smem)
   flush_counts(T.cnt, seg, node, tc, real, fail);
 }
 
-/* Saved paths of live list 0, resumed by the sorted finishing kernel: a
- * warp takes its idle lanes' entries with one atomic; the lane past the end
- * of the list marks it exhausted */
-struct ResumeLive {
-  static constexpr bool kActive = true;
-  const uint4* paths;
-  const uint32_t* list0;
-  WCtl* ctl;
-  uint32_t n;
-  __device__ __forceinline__ bool
-  take(Path& p, bool want, unsigned lane, uint32_t* exhausted) const
-  {
-    const unsigned m = __ballot_sync(0xffffffffu, want);
-    if(!m) return false;
-    const unsigned leader = __ffs(m) - 1;
-    uint32_t i0 = 0;
-    if(lane == leader) i0 = atomicAdd(&ctl->fetch_finish, (uint32_t)__popc(m));
-    i0 = __shfl_sync(0xffffffffu, i0, leader);
-    if(!want) return false;
-    const uint32_t idx = i0 + __popc(m & ((1u << lane) - 1u));
-    if(idx >= n) { *exhausted = 1; return false; }
-    load_path(p, paths + (size_t)list0[idx] * kPathV4);
-    p.t0 = gtimer() - p.t0; /* stored: busy time so far */
-    return true;
-  }
-};
-
-/* The tail on the block-sorted loop: the saved paths of live list 0 and then
- * the queue, run from shared-memory slots regrouped by stage over the whole
- * block at every step */
-template <unsigned V>
-__global__ void __maxnreg__(HG_PERSIST_MAXNREG)
-k_wave_finish_sorted(WTables W, int tables_in_smem)
-{
-  extern __shared__ __align__(16) unsigned char smem[];
-  PTables T = W.T;
-  PathSlot* slots = (PathSlot*)smem;
-  uint32_t* lists = (uint32_t*)(smem + path_slots_bytes(blockDim.x));
-  if(tables_in_smem)
-    tables_to_smem(T, smem + path_slots_bytes(blockDim.x) + sorted_lists_bytes(blockDim.x));
-  const ResumeLive src{W.paths, W.list0, W.ctl, W.ctl->n_live[0]};
-  sorted_loop<V>(T, slots, lists, src);
-}
-
 size_t
 wave_slot_bytes()
 {
@@ -491,17 +441,13 @@ wave_event_fn(uint32_t v)
 WaveFinishFn
 wave_finish_fn(uint32_t v)
 {
-#if HG_WAVE_SORTED_TAIL
-  HG_PICK_VARIANT(v, k_wave_finish_sorted)
-#else
   HG_PICK_VARIANT(v, k_wave_finish)
-#endif
 }
 
 /* Launch shapes of a run over the tables T */
 struct WaveLaunch {
   size_t smem = 0;
-  size_t fi_smem = 0; /* of the finishing kernel (its path slots when sorted) */
+  size_t fi_smem = 0; /* of the finishing kernel */
   int in_smem = 0;
   unsigned ev_grid = 0, tr_grid = 0, fi_grid = 0;
   uint32_t tb = 256;
@@ -521,12 +467,7 @@ wave_params(const PTables& T, const htrdr_gpu_tuning& tun, int device, WaveLaunc
   L.ev = wave_event_fn(T.variant);
   L.fi = wave_finish_fn(T.variant);
   L.tb = tun.block_size ? tun.block_size : 256;
-#if HG_WAVE_SORTED_TAIL
-  L.fi_smem = L.smem + path_slots_bytes(L.tb) + sorted_lists_bytes(L.tb);
-  if(L.fi_smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-#else
   L.fi_smem = L.smem;
-#endif
   cudaError_t e;
   if(L.smem > 48 * 1024) {
     if((e = cudaFuncSetAttribute(L.ev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem)))
