@@ -93,6 +93,11 @@ struct DScene {
   uint32_t depth;
   const uint4* nodes;     /* node pool */
   const uint64_t* tree_base; /* [nq*3]: first node of the octree (q, prop) */
+  /* leaf of every cell of every octree, (node index in its tree) << 5 | level:
+   * grid `grid_rank[q*3+prop]' of ncell entries; null when it did not fit */
+  const uint32_t* leaf_grid;
+  const uint32_t* grid_rank; /* [nq*3] */
+  uint64_t ncell;            /* def[0] * def[1] * def[2] */
   /* ground */
   int32_t has_ground, ground_brdf;
   float ground_refl, ground_T;

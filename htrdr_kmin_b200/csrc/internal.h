@@ -114,6 +114,11 @@ void build_octree(const DScene& hs, const float* lwc, const float* sig3, const f
                   uint32_t depth, uint32_t level_force, double tau, double cmax,
                   std::vector<uint32_t>& nodes);
 
+/* Leaf of every cell of every built octree (octree_gpu.cu): false when the
+ * grids do not fit or cannot be indexed (the traversal then descends) */
+bool build_leaf_grids(const DScene& S, const std::vector<uint64_t>& tree_base,
+                      const std::vector<uint64_t>& tree_count, DevBuf& grids, std::vector<uint32_t>& rank);
+
 /* Ground mesh: validation, BVH and device tables into S (ground.cpp);
  * `upload' copies a host array to a device buffer owned by the scene */
 htrdr_gpu_res_T setup_ground_mesh(const htrdr_gpu_scene_desc* desc, DScene& S,

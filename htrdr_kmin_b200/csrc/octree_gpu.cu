@@ -151,7 +151,56 @@ k_emit(const Entry* __restrict__ list, uint32_t count, LevelDims dims, const flo
 inline unsigned
 grid_of(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
 
+/* Leaf of every cell of one tree: a descent from the root by the cell's
+ * coordinate bits, written as (node index in the tree) << 5 | level */
+__global__ void
+k_leafgrid(const uint4* __restrict__ nodes, uint32_t depth, uint32_t nx, uint32_t ny, uint32_t nz,
+           uint32_t* grid)
+{
+  const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if(c >= (uint64_t)nx * ny * nz) return;
+  const uint32_t x = (uint32_t)(c % nx), y = (uint32_t)((c / nx) % ny), z = (uint32_t)(c / ((uint64_t)nx * ny));
+  uint32_t n = 0, L = depth;
+  uint32_t child = nodes[0].z;
+  while(child != HG_LEAF && L > 0) {
+    --L;
+    n = child + (((x >> L) & 1u) | (((y >> L) & 1u) << 1) | (((z >> L) & 1u) << 2));
+    child = nodes[n].z;
+  }
+  grid[c] = (n << 5) | L;
+}
+
 }  // namespace
+
+/* Leaf grids of the built trees (tree_count[i] > 0, in index order) into
+ * `grids'; rank[i] is the grid of tree i.  Returns false (no grid built, no
+ * error) when they would not fit in half of the free device memory or a tree
+ * is too large for the 27-bit node index of an entry. */
+bool
+build_leaf_grids(const DScene& S, const std::vector<uint64_t>& tree_base,
+                 const std::vector<uint64_t>& tree_count, DevBuf& grids, std::vector<uint32_t>& rank)
+{
+  const uint64_t ncell = (uint64_t)S.def[0] * S.def[1] * S.def[2];
+  rank.assign(tree_base.size(), 0);
+  uint32_t ntrees = 0;
+  for(size_t i = 0; i < tree_count.size(); ++i) {
+    if(!tree_count[i]) continue;
+    if(tree_count[i] >= (1ull << 27)) return false;
+    rank[i] = ntrees++;
+  }
+  if(!ntrees || !ncell) return false;
+  size_t free_b = 0, total_b = 0;
+  if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
+  const uint64_t bytes = (uint64_t)ntrees * ncell * 4;
+  if(bytes > free_b / 2) return false;
+  if(!grids.alloc(bytes)) return false;
+  for(size_t i = 0; i < tree_count.size(); ++i) {
+    if(!tree_count[i]) continue;
+    k_leafgrid<<<grid_of(ncell, 256), 256>>>(S.nodes + tree_base[i], S.depth, S.def[0], S.def[1],
+                                              S.def[2], (uint32_t*)grids.ptr + (uint64_t)rank[i] * ncell);
+  }
+  return cuda_ok(cudaGetLastError(), "leaf grids") && cuda_ok(cudaDeviceSynchronize(), "leaf grids");
+}
 
 /* Scratch and stream of one build worker: the level arrays of one tree, the
  * depth lists of its emission and the scan's temporary storage */

@@ -19,6 +19,11 @@
 #include <string>
 #include <thread>
 
+/* Leaf grids of the octrees (1: built when they fit; 0: never) */
+#ifndef HG_LEAF_GRID
+#define HG_LEAF_GRID 1
+#endif
+
 namespace hg {
 
 static thread_local std::string g_last_error;
@@ -895,6 +900,18 @@ scene_create(int device, const htrdr_gpu_scene_desc* desc, const char* cache_pat
     }
     if(!(S.tree_base = (const uint64_t*)upload(scn->tree_base.data(), scn->tree_base.size() * 8)))
       return HTRDR_GPU_RES_MEM_ERR;
+    S.ncell = (uint64_t)S.def[0] * S.def[1] * S.def[2];
+    auto grids = std::make_unique<DevBuf>();
+    std::vector<uint32_t> rank;
+    if(HG_LEAF_GRID && build_leaf_grids(S, scn->tree_base, scn->tree_count, *grids, rank)) {
+      if(!(S.grid_rank = (const uint32_t*)upload(rank.data(), rank.size() * 4)))
+        return HTRDR_GPU_RES_MEM_ERR;
+      S.leaf_grid = (const uint32_t*)grids->ptr;
+      scn->bytes += grids->bytes;
+      scn->bufs.push_back(std::move(grids));
+    } else {
+      cudaGetLastError(); /* an allocation refused for the optional grids is not an error */
+    }
   }
 
   S.has_ground = desc->has_ground ? 1 : 0;

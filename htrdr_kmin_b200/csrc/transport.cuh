@@ -423,6 +423,7 @@ struct Trace {
   float ta, cb0, cb1, tb;  /* regions: gas [ta,cb0) | cloud [cb0,cb1) | gas [cb1,tb) */
   float t;                 /* start of the current voxel */
   float tcur;              /* traversal distance (filter context) */
+  uint32_t grank;          /* leaf grid of the octree (cloud region) */
   double Ts, Tmin;
   uint64_t base;           /* first node of the octree */
   int32_t layer;           /* gas region: current layer */
@@ -603,6 +604,7 @@ trace_begin(Path& p, const DScene& S, int kind, int prop, float3 o, float3 d, fl
       T.cb0 = c0;
       T.cb1 = c1;
       T.base = S.tree_base[(size_t)p.q * 3 + prop];
+      T.grank = S.leaf_grid ? __ldg(S.grid_rank + (size_t)p.q * 3 + prop) : 0u;
     }
   }
   region_enter(T, S);
@@ -822,8 +824,27 @@ trace_step(Path& p, const DScene& S)
   uint32_t L, base;
   uint4 v;
   bool leaf_root = false;
+  bool found = false;
   if(T.start == 1) {
     base = T.p_base; L = T.p_level;
+  } else if(S.leaf_grid) {
+    /* the leaf from the cell's grid entry: two dependent loads whatever the
+     * depth; its parent's child block is cached for the next steps */
+    const uint64_t cell = ((uint64_t)T.c[2] * S.def[1] + T.c[1]) * S.def[0] + T.c[0];
+    const uint32_t e = __ldg(S.leaf_grid + (uint64_t)T.grank * S.ncell + cell);
+    const uint32_t n = e >> 5;
+    L = e & 31u;
+    v = __ldg(nodes + n);
+    ++p.c_node;
+    found = true;
+    if(L < S.depth) {
+      const uint32_t oct = ((T.c[0] >> L) & 1u) | (((T.c[1] >> L) & 1u) << 1) | (((T.c[2] >> L) & 1u) << 2);
+      T.p_base = n - oct;
+      T.p_level = (uint8_t)(L + 1);
+    } else {
+      T.p_level = 0xFF; /* the root is the leaf: no ancestor */
+    }
+    T.g_level = 0xFF;
   } else if(T.start == 2) {
     base = T.g_base; L = T.g_level;
     T.p_base = base; T.p_level = (uint8_t)L; T.g_level = 0xFF;
@@ -835,7 +856,7 @@ trace_step(Path& p, const DScene& S)
     T.p_base = base; T.p_level = (uint8_t)L; T.g_level = 0xFF;
     leaf_root = v.z == HG_LEAF;
   }
-  if(!leaf_root) {
+  if(!leaf_root && !found) {
     for(;;) {
       --L;
       const uint32_t oct = ((T.c[0] >> L) & 1u) | (((T.c[1] >> L) & 1u) << 1) | (((T.c[2] >> L) & 1u) << 2);
@@ -846,7 +867,7 @@ trace_step(Path& p, const DScene& S)
       T.p_base = v.z; T.p_level = (uint8_t)L;
       base = v.z;
     }
-  } else {
+  } else if(leaf_root) {
     T.p_level = 0xFF; /* the root is the leaf: no ancestor */
   }
   uint32_t lo[3], hi[3];
