@@ -649,7 +649,7 @@ class Setup:
 
 
 def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: int, world: int,
-            dist, clocks: bool = True) -> dict:
+            dist, clocks: bool = True, traffic_key: str = "") -> dict:
     """Batched launches of the whole workload (warm-up, then `steps' timed
     launches), the plain drop-in one request at a time, and the e2e call with
     host buffers.  Returns the JSON fields of the workload."""
@@ -767,7 +767,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kms * 1e-3) / 1e9
     kernel = "wavefront" if wave else ("k_sorted" if tuning.engine == api.ENGINE_SORTED else "k_persistent")
-    traffic, traffic_src = traffic_per_launch(kernel, alg_bytes)
+    traffic, traffic_src = traffic_per_launch(traffic_key or kernel, alg_bytes)
     out_bytes = sum(d.numel() for d in su.dev)
     line = {
         "value": world * reals / (step_ms * 1e-3) / 1e6, "ms_per_step": step_ms,
@@ -857,7 +857,9 @@ def main():
         su.close()
         return
     tuning, src = pick_tuning(args, api, su, args.workload)
-    fields, gpu_maps, _ = measure(args, api, su, desc, tuning, src, rank, world, dist)
+    fields, gpu_maps, _ = measure(args, api, su, desc, tuning, src, rank, world, dist,
+                                  traffic_key="wavefront_lw" if (args.workload == "lw_flux"
+                                                                 and tuning.engine == api.ENGINE_WAVEFRONT) else "")
 
     line = {"metric": METRIC, "value": fields.pop("value"), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": fields.pop("ms_per_step"),
@@ -899,7 +901,8 @@ def main():
         su2 = Setup(api, [sc2], [(0, rq2)], local)
         t2, src2 = pick_tuning(args, api, su2, "lw_flux") if not args.tuning else (
             api.mode_tuning(S.MODE_FLUX_LW), "mode default")
-        f2, _, _ = measure(args, api, su2, desc2, t2, src2, rank, world, dist, clocks=False)
+        f2, _, _ = measure(args, api, su2, desc2, t2, src2, rank, world, dist, clocks=False,
+                           traffic_key="wavefront_lw" if t2.engine == api.ENGINE_WAVEFRONT else "")
         line["lw_flux"] = {k: f2[k] for k in ("value", "ms_per_step", "e2e", "plain_gpu",
                                               "batched_vs_plain", "roofline", "segments_per_s")}
         line["lw_flux"]["unit"] = UNIT
