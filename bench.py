@@ -557,6 +557,14 @@ def run_serve(args):
         g.close()
 
 
+def alg_bytes_of(st) -> int:
+    """Algorithmic bytes of a launch from its counters: 16 per majorant node
+    fetched, 4 per leaf-grid entry read, 8 per tentative collision (its
+    raw-property gather: cloud cell and gas layer) and 32 per realisation (the
+    read-modify-write of its FP64 sums and count)."""
+    return 16 * st.nodes + 4 * st.grid_lookups + 8 * st.collisions + 32 * st.realisations
+
+
 def traffic_per_launch(kernel: str, alg_bytes: int):
     """DRAM bytes of one launch of `kernel', from the ncu capture summarised
     in profiles/traffic.json: dram__bytes_read.sum + dram__bytes_write.sum of
@@ -763,7 +771,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     wave = tuning.engine == api.ENGINE_WAVEFRONT
     reals = last.realisations
     kms = float(np.mean(kernel_ms))
-    alg_bytes = 16 * last.nodes + 8 * last.collisions + 32 * last.realisations
+    alg_bytes = alg_bytes_of(last)
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kms * 1e-3) / 1e9
     kernel = "wavefront" if wave else ("k_sorted" if tuning.engine == api.ENGINE_SORTED else "k_persistent")
@@ -792,7 +800,8 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
                       "kernel_ms": plain_ms, "launches": n},
         "batched_vs_plain": plain_ms / kms,
         "segments_per_s": last.segments / (kms * 1e-3),
-        "counters": {"segments": last.segments, "nodes": last.nodes, "collisions": last.collisions,
+        "counters": {"segments": last.segments, "nodes": last.nodes,
+                     "grid_lookups": last.grid_lookups, "collisions": last.collisions,
                      "realisations": last.realisations, "failures": last.failures},
     }
     if sampler:
@@ -848,10 +857,11 @@ def main():
         res = api.lib().htrdr_gpu_draw_maps_batched_device(su.items_dev, su.n, C.byref(tuning), C.byref(st))
         if res != 0:
             raise api.HtrdrError("batched_device", res, api.lib().htrdr_gpu_last_error().decode())
-        alg = 16 * st.nodes + 8 * st.collisions + 32 * st.realisations
+        alg = alg_bytes_of(st)
         print(json.dumps({"workload": desc, "tuning": tuning_dict(tuning, "command line"),
                           "kernel_ms": st.kernel_ms, "launches": st.launches, "alg_bytes": alg,
                           "counters": {"segments": st.segments, "nodes": st.nodes,
+                                       "grid_lookups": st.grid_lookups,
                                        "collisions": st.collisions, "realisations": st.realisations}}),
               flush=True)
         su.close()

@@ -81,6 +81,7 @@ persistent_loop(PTables& T, Path& p)
         trace_step<V>(p, S);
       } else if(p.state == ST_DONE) {
         accumulate_b(p, R);
+        count_grid(T.cnt, p);
         real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
         fail += (p.flags & PF_FAILED) ? 1 : 0;
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;
@@ -364,12 +365,12 @@ plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_g
 }
 
 static void
-read_stats(const unsigned long long c[5], float kms, float tms, uint64_t launches,
+read_stats(const unsigned long long c[6], float kms, float tms, uint64_t launches,
            htrdr_gpu_stats* stats)
 {
   if(!stats) return;
   stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
-  stats->realisations = c[3]; stats->failures = c[4];
+  stats->realisations = c[3]; stats->failures = c[4]; stats->grid_lookups = c[5];
   stats->kernel_ms = kms; stats->total_ms = tms;
   stats->launches = launches;
 }
@@ -452,7 +453,7 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
   cudaEventRecord(e0, st);
   bool ok = plan_enqueue(P, items, n, tun, host, st, e1, e2);
   cudaEventRecord(e3, st);
-  unsigned long long c[5] = {0, 0, 0, 0, 0};
+  unsigned long long c[6] = {0, 0, 0, 0, 0, 0};
   if(ok) ok = cuda_ok(cudaMemcpyAsync(c, P.d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H");
   if(ok) ok = cuda_ok(cudaStreamSynchronize(st), "sync");
   if(ok) {
@@ -608,7 +609,7 @@ htrdr_gpu_batch_run(htrdr_gpu_batch* b, htrdr_gpu_stats* stats)
 try {
   if(!b) return HTRDR_GPU_RES_BAD_ARG;
   cudaSetDevice(b->plan.device);
-  unsigned long long c[5] = {0, 0, 0, 0, 0};
+  unsigned long long c[6] = {0, 0, 0, 0, 0, 0};
   bool ok = cuda_ok(cudaEventRecord(b->e0, b->stream), "event")
          && cuda_ok(cudaGraphLaunch(b->exec, b->stream), "graph launch")
          && cuda_ok(cudaEventRecord(b->e3, b->stream), "event")

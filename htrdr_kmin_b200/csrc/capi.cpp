@@ -90,7 +90,7 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   if(ok && host)
     ok = cuda_ok(cudaMemcpyAsync(buffer, dout, out_bytes, cudaMemcpyDeviceToHost, st), "D2H");
   cudaEventRecord(e3, st);
-  unsigned long long c[5] = {0, 0, 0, 0, 0};
+  unsigned long long c[6] = {0, 0, 0, 0, 0, 0};
   if(ok) ok = cuda_ok(cudaMemcpyAsync(c, ws.cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H");
   if(ok) ok = cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   if(ok && stats) {
@@ -98,7 +98,7 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
     cudaEventElapsedTime(&k, e1, e2);
     cudaEventElapsedTime(&t, e0, e3);
     stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
-    stats->realisations = c[3]; stats->failures = c[4];
+    stats->realisations = c[3]; stats->failures = c[4]; stats->grid_lookups = c[5];
     stats->kernel_ms = k; stats->total_ms = t;
     stats->launches = take_launches();
   }

@@ -149,6 +149,14 @@ flush_counts(void* cnt, unsigned long long seg, unsigned long long node, unsigne
   }
 }
 
+/* Leaf-grid lookups of a completed path, added to the launch's total: one
+ * atomic per realisation, so that no engine keeps another running counter */
+__device__ __forceinline__ void
+count_grid(void* cnt, const Path& p)
+{
+  if(p.c_grid) atomicAdd(&((Counters*)cnt)->grid, (unsigned long long)p.c_grid);
+}
+
 /* Copy the scene and request tables of a launch into shared memory (one
  * copy per block) and point T at them */
 /* A path held in shared memory.  8 bytes of padding give an odd number of
@@ -265,6 +273,7 @@ sorted_loop(hg::PTables& T, PathSlot* slots, uint32_t* lists)
       Path& p = slots[act ? event_list[tid] : 0].p;
       if(act && p.state == ST_DONE) {
         accumulate_b(p, T.reqs[p.ri]);
+        count_grid(T.cnt, p);
         real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
         fail += (p.flags & PF_FAILED) ? 1 : 0;
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;

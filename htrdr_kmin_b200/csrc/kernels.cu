@@ -81,6 +81,7 @@ k_plain(DScene S, DRequest R, DAccum* acc, DAccum* tacc, uint64_t pix_begin, uin
       accumulate(p, R, acc, tacc);
     }
     seg = p.c_seg; node = p.c_node; tc = p.c_tc;
+    if(cnt && p.c_grid) atomicAdd(&cnt->grid, (unsigned long long)p.c_grid);
     real = (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
     fail = (p.flags & PF_FAILED) ? 1 : 0;
   }

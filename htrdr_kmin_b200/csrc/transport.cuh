@@ -455,7 +455,7 @@ enum {
 };
 
 struct Counters {
-  unsigned long long seg, node, tc, real, fail;
+  unsigned long long seg, node, tc, real, fail, grid;
 };
 
 struct Path {
@@ -463,6 +463,8 @@ struct Path {
    * that the wavefront engine's trace stage moves only this prefix of a
    * stored path (HG_TRACE_WORDS). */
   Rng rng;
+  uint32_t c_grid;      /* local counter of leaf-grid lookups (the word before
+                         * the 8-byte aligned Trace: no extra storage) */
   Trace tr;
   uint32_t band, q, flags;
   uint32_t si;          /* scene of the path (engines with many scenes) */
@@ -487,6 +489,7 @@ struct Path {
 /* 32-bit words of a stored path, and of its trace part */
 #define HG_PATH_WORDS ((uint32_t)(sizeof(Path) / 4))
 #define HG_TRACE_WORDS ((uint32_t)(offsetof(Path, org) / 4))
+static_assert(offsetof(Path, tr) == 40 && offsetof(Path, org) == 224, "trace prefix of 56 words");
 static_assert(sizeof(Path) % 4 == 0 && offsetof(Path, org) % 4 == 0, "word-wise path storage");
 
 __device__ __forceinline__ unsigned long long
@@ -836,6 +839,7 @@ trace_step(Path& p, const DScene& S)
     L = e & 31u;
     v = __ldg(nodes + n);
     ++p.c_node;
+    ++p.c_grid;
     found = true;
     if(L < S.depth) {
       const uint32_t oct = ((T.c[0] >> L) & 1u) | (((T.c[1] >> L) & 1u) << 1) | (((T.c[2] >> L) & 1u) << 2);
@@ -1103,7 +1107,7 @@ path_generate(Path& p, const DScene& S, const DRequest& R)
   const GenOut g = gen_sample(S, R, p.pix, p.ireal);
   p.w = 0.0;
   p.wdirect = 0.0;
-  p.c_seg = p.c_node = p.c_tc = 0;
+  p.c_seg = p.c_node = p.c_tc = p.c_grid = 0;
   p.t0 = gtimer();
   p.rng = g.rng;
   p.chan = (uint8_t)g.chan;

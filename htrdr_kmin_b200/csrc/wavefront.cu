@@ -152,6 +152,7 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
         }
         if(p.state == ST_DONE) {
           accumulate_b(p, T.reqs[p.ri]);
+          count_grid(T.cnt, p);
           real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
           fail += (p.flags & PF_FAILED) ? 1 : 0;
           p.state = ST_IDLE;
@@ -373,6 +374,7 @@ k_wave_finish(WTables W, int tables_in_smem)
         trace_step<V>(p, S);
       } else if(p.state == ST_DONE) {
         accumulate_b(p, R);
+        count_grid(T.cnt, p);
         real += (p.flags & (PF_REJECTED | PF_FAILED)) ? 0 : 1;
         fail += (p.flags & PF_FAILED) ? 1 : 0;
         seg += p.c_seg; node += p.c_node; tc += p.c_tc;

@@ -141,6 +141,8 @@ struct htrdr_gpu_stats {
   double kernel_ms;      /* CUDA-event time of the transport kernel(s) */
   double total_ms;       /* whole call, device side */
   uint64_t launches;     /* kernels the call launched (transport, initialisation, finalize) */
+  uint64_t grid_lookups; /* leaf-grid entries read (4 bytes each; every one is
+                          * followed by one of the `nodes' fetches) */
 };
 
 struct htrdr_gpu_scene;

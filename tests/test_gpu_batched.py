@@ -71,6 +71,7 @@ def test_wavefront_equals_plain(gpu_lib, slots, budget, bs, tail):
     ref, sref = gpu_lib.draw_maps_batched(items, gpu_lib.default_tuning())
     assert st["realisations"] == sref["realisations"]
     assert st["segments"] == sref["segments"] and st["collisions"] == sref["collisions"]
+    assert st["nodes"] == sref["nodes"] and st["grid_lookups"] == sref["grid_lookups"]
     for (gs, req), b, r in zip(items, bufs, ref):
         gs.set_engine(gpu_lib.ENGINE_PLAIN)
         p, _ = gs.draw_map(req)
@@ -101,6 +102,7 @@ def test_draw_map_engines_agree(gpu_lib):
     """htrdr_gpu_draw_map on the persistent engine (default, by-mode or given
     tuning) equals the plain engine, on host and device outputs."""
     import torch
+    lookups = 0
     for gs, req in _mix(gpu_lib):
         gs.set_engine(gpu_lib.ENGINE_PLAIN)
         plain, sp = gs.draw_map(req)
@@ -117,6 +119,12 @@ def test_draw_map_engines_agree(gpu_lib):
         wave, sw = gs.draw_map(req)
         _cmp(wave, plain, req.mode)
         assert sw["segments"] == sp["segments"]
+        # every path takes the same voxel steps on every engine, so it reads
+        # the same leaf-grid entries, each followed by one node fetch
+        assert sp["grid_lookups"] == spp["grid_lookups"] == sw["grid_lookups"]
+        assert sp["nodes"] == spp["nodes"] == sw["nodes"]
+        assert sp["grid_lookups"] <= sp["nodes"]
+        lookups += sp["grid_lookups"]
         t.trace_budget, t.wave_slots, t.wave_tail = 5, 333, 100
         gs.set_engine(gpu_lib.ENGINE_WAVEFRONT, t)
         wave2, _ = gs.draw_map(req)
@@ -127,6 +135,7 @@ def test_draw_map_engines_agree(gpu_lib):
         got = np.frombuffer(dev.cpu().numpy().tobytes(), dtype=pers.dtype).reshape(pers.shape)
         _cmp(got, plain, req.mode)
         gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
+    assert lookups > 0
     gs, req = _mix(gpu_lib)[0]
     bad = gpu_lib.default_tuning()
     bad.block_size = 48  # not a multiple of a warp
