@@ -38,43 +38,63 @@ constexpr uint32_t kPathV4 = (uint32_t)((sizeof(Path) + 15) / 16);
 constexpr uint32_t kTraceV4 = (uint32_t)((offsetof(Path, org) + 15) / 16);
 static_assert(kTraceV4 <= kPathV4, "trace part inside the path");
 
+/* Slot storage: a path is kPathV4 16-byte vectors.  HG_WAVE_SOA 0 (default)
+ * keeps a slot's vectors contiguous (a lane reading its own slot uses every
+ * byte of the sectors it touches, whatever slots its warp holds); 1 stores
+ * vector i of every slot together (coalesced only when a warp's slots are
+ * consecutive). */
+#ifndef HG_WAVE_SOA
+#define HG_WAVE_SOA 0
+#endif
+
+__device__ __forceinline__ size_t
+vec_at(uint32_t s, uint32_t i, uint32_t P)
+{
+#if HG_WAVE_SOA
+  return (size_t)i * P + s;
+#else
+  (void)P;
+  return (size_t)s * kPathV4 + i;
+#endif
+}
+
 __device__ __forceinline__ void
-load_path(Path& p, const uint4* src)
+load_path(Path& p, const uint4* paths, uint32_t s, uint32_t P)
 {
   uint4 v[kPathV4];
 #pragma unroll
-  for(uint32_t i = 0; i < kPathV4; ++i) v[i] = src[i];
+  for(uint32_t i = 0; i < kPathV4; ++i) v[i] = paths[vec_at(s, i, P)];
   memcpy(&p, v, sizeof(Path));
 }
 
 __device__ __forceinline__ void
-store_path(const Path& p, uint4* dst)
+store_path(const Path& p, uint4* paths, uint32_t s, uint32_t P)
 {
   uint4 v[kPathV4];
   v[kPathV4 - 1] = make_uint4(0, 0, 0, 0);
   memcpy(v, &p, sizeof(Path));
 #pragma unroll
-  for(uint32_t i = 0; i < kPathV4; ++i) dst[i] = v[i];
+  for(uint32_t i = 0; i < kPathV4; ++i) paths[vec_at(s, i, P)] = v[i];
 }
 
 /* The trace part and the bytes up to the next 16-byte boundary (stored back
  * unchanged) */
 __device__ __forceinline__ void
-load_trace(Path& p, const uint4* src)
+load_trace(Path& p, const uint4* paths, uint32_t s, uint32_t P)
 {
   uint4 v[kTraceV4];
 #pragma unroll
-  for(uint32_t i = 0; i < kTraceV4; ++i) v[i] = src[i];
+  for(uint32_t i = 0; i < kTraceV4; ++i) v[i] = paths[vec_at(s, i, P)];
   memcpy(&p, v, kTraceV4 * 16);
 }
 
 __device__ __forceinline__ void
-store_trace(const Path& p, uint4* dst)
+store_trace(const Path& p, uint4* paths, uint32_t s, uint32_t P)
 {
   uint4 v[kTraceV4];
   memcpy(v, &p, kTraceV4 * 16);
 #pragma unroll
-  for(uint32_t i = 0; i < kTraceV4; ++i) dst[i] = v[i];
+  for(uint32_t i = 0; i < kTraceV4; ++i) paths[vec_at(s, i, P)] = v[i];
 }
 
 }  // namespace
@@ -82,7 +102,7 @@ store_trace(const Path& p, uint4* dst)
 /* Control block of a wavefront run (device) */
 struct WTables {
   PTables T;
-  uint4* paths;     /* [P][kPathV4] */
+  uint4* paths;     /* P slots of kPathV4 vectors (vec_at) */
   uint32_t* list0;  /* live lists, P entries each */
   uint32_t* list1;
   uint32_t* dead;   /* free slots (serving: revived when work arrives), or null */
@@ -117,11 +137,10 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
     const uint32_t idx = base + lane;
     const bool active = idx < n_in;
     const uint32_t s = active ? in[idx] : 0u;
-    uint4* slot = W.paths + (size_t)s * kPathV4;
     Path p;
     p.state = ST_IDLE;
     if(active) {
-      load_path(p, slot);
+      load_path(p, W.paths, s, W.P);
       p.t0 = gtimer() - p.t0; /* stored: busy time so far */
     }
     bool drained = !active;
@@ -162,7 +181,7 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
     const bool keep = p.state == ST_TRACE;
     if(keep) {
       p.t0 = gtimer() - p.t0;
-      store_path(p, slot);
+      store_path(p, W.paths, s, W.P);
     }
     const unsigned km = __ballot_sync(0xffffffffu, keep);
     if(km) {
@@ -173,7 +192,7 @@ k_wave_event(WTables W, uint32_t b, int tables_in_smem)
     }
     /* serving: a slot left without work waits, idle, on the dead list */
     const bool died = active && !keep && W.dead;
-    if(died) store_path(p, slot); /* p.state is ST_IDLE */
+    if(died) store_path(p, W.paths, s, W.P); /* p.state is ST_IDLE */
     const unsigned dm = __ballot_sync(0xffffffffu, died);
     if(dm) {
       uint32_t pos = 0;
@@ -216,7 +235,7 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
         const uint32_t idx = i0 + __popc(m & ((1u << lane) - 1u));
         if(idx < n) {
           s = list[idx];
-          load_trace(p, W.paths + (size_t)s * kPathV4);
+          load_trace(p, W.paths, s, W.P);
           p.t0 = gtimer() - p.t0;
           have = true;
           left = W.budget;
@@ -230,7 +249,7 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
       trace_step<HV_ALL>(p, T.scenes[p.si]);
       if(p.state != ST_TRACE || --left == 0) {
         p.t0 = gtimer() - p.t0;
-        store_trace(p, W.paths + (size_t)s * kPathV4);
+        store_trace(p, W.paths, s, W.P);
         have = false;
       }
     }
@@ -339,7 +358,7 @@ k_wave_finish(WTables W, int tables_in_smem)
       if(need_l) {
         const uint32_t idx = i0 + __popc(ml & ((1u << lane) - 1u));
         if(idx < n) {
-          load_path(p, W.paths + (size_t)W.list0[idx] * kPathV4);
+          load_path(p, W.paths, W.list0[idx], W.P);
           p.t0 = gtimer() - p.t0;
         } else {
           list_done = true;
