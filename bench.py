@@ -10,8 +10,10 @@ realisations so that one step takes seconds (at full ranges one request holds
 up to 10^9 realisations).  A step renders the whole mix.
 
 * value: Mrealisations/s of the mix rendered in one launch of the work-queue
-  engine the autotuner picks, outputs in HBM, scenes resident; device time
-  from CUDA events on the library's stream, max over ranks.
+  engine the autotuner picks (its wavefront tail threshold timed on the full
+  mix), outputs in HBM, scenes resident; the K steps timed between two CUDA
+  events that bracket them (the host's share of each call included), max
+  over ranks.
 * plain_gpu / batched_vs_plain: the same requests one at a time through the
   plain engine of the drop-in (one thread per realisation).
 * serving: the same requests arriving as a Poisson process at a rate that
@@ -37,8 +39,8 @@ Other workloads (development and profiling): ``lw_flux``, ``sw_image``,
 scale) and ``serve`` (a sweep of arrival rates on that mix).
 
 Multi-GPU (torchrun): every rank renders the whole workload with its own
-random streams (weak scaling); the flux maps' per-probe FP64 accumulators are
-summed on rank 0 with NCCL.
+random streams (weak scaling); every map's FP64 accumulators are summed on
+rank 0 with NCCL and finalized there.
 """
 from __future__ import annotations
 
@@ -742,12 +744,19 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     if sampler:
         sampler.__enter__()
     barrier()
+    # the K steps between two events on the device: each call returns after
+    # its work is done, so the span also holds the host's share of every call
+    # (plan building, launches, waits) and the gaps between calls
+    span0, span1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    span0.record()
     for _ in range(args.steps):
         st, red = step_batched()
         kernel_ms.append(st.kernel_ms)
         total_ms.append(st.total_ms + red)
         stats.append(st)
+    span1.record()
     barrier()
+    span_ms = span0.elapsed_time(span1)
     if sampler:
         sampler.__exit__(None, None, None)
     gpu_maps = su.host_maps() if rank == 0 else None
@@ -761,7 +770,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     barrier()
     e2e_ms = 1e3 * (time.perf_counter() - t0) / e2e_steps
 
-    step_ms = float(np.sum(total_ms)) / args.steps
+    step_ms = span_ms / args.steps
     if dist is not None:
         t = torch.tensor([step_ms, e2e_ms], device=f"cuda:{su.local}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -779,6 +788,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     out_bytes = sum(d.numel() for d in su.dev)
     line = {
         "value": world * reals / (step_ms * 1e-3) / 1e6, "ms_per_step": step_ms,
+        "call_device_ms_per_step": float(np.mean(total_ms)),
         "config": {"workload": desc, "realisations_per_step_per_gpu": int(su.total_real),
                    "tuning": tuning_dict(tuning, tuning_src),
                    "l2": "inputs larger than L2: scenes of "
@@ -809,17 +819,36 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
     return line, gpu_maps, stats
 
 
+TAILS = (25000, 50000, 100000, 200000)
+
+
 def pick_tuning(args, api, su: "Setup", name: str):
     """Tuning of the batched engine: the command line's, else the autotuner's
     (on the mix at 1/8 of its realisations per pixel for mix_full, so that its
-    28 candidate runs stay short)."""
+    28 candidate runs stay short).  The tail threshold of a wavefront pick is
+    then timed on the full mix: at 1/8 of the work the longest walks, which
+    the threshold is about, weigh eight times as much."""
     if args.tuning:
         return parse_tuning(api, args.tuning), "command line"
-    if name == "mix_full":
-        tuning, _ = api.autotune(su.reduced_items(8))
-        return tuning, "autotuner (on the same mix at 1/8 of the realisations per pixel)"
-    tuning, _ = api.autotune(su.items_dev)
-    return tuning, "autotuner"
+    if name != "mix_full":
+        tuning, _ = api.autotune(su.items_dev)
+        return tuning, "autotuner"
+    tuning, _ = api.autotune(su.reduced_items(8))
+    src = "autotuner (on the same mix at 1/8 of the realisations per pixel)"
+    if tuning.engine != api.ENGINE_WAVEFRONT:
+        return tuning, src
+    L = api.lib()
+    best = None
+    for tail in TAILS:
+        t = api.Tuning(*[getattr(tuning, f) for f, _ in api.Tuning._fields_])
+        t.wave_tail = tail
+        st = api.Stats()
+        res = L.htrdr_gpu_draw_maps_batched_device(su.items_dev, su.n, C.byref(t), C.byref(st))
+        if res != 0:
+            raise api.HtrdrError("batched_device", res, L.htrdr_gpu_last_error().decode())
+        if best is None or st.kernel_ms < best[0]:
+            best = (st.kernel_ms, t)
+    return best[1], src + f", tail threshold timed on the full mix ({', '.join(map(str, TAILS))})"
 
 
 def main():

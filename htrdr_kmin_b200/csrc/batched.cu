@@ -256,7 +256,7 @@ struct Plan {
   bool accum_out = false; /* the items' buffers receive the accumulators */
   std::vector<size_t> item_acc_bytes;
   PTables T{};
-  WaveBufs wave; /* path slots of the wavefront engine */
+  WaveBufs* wave = nullptr; /* path slots of the wavefront engine (the thread's pool) */
 };
 
 static htrdr_gpu_res_T
@@ -275,6 +275,7 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out,
   P.accum_out = accum_out;
   if(!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
   P.device = device;
+  P.wave = &thread_wave(device);
   P.reqs.resize(n);
   P.items.resize(n);
   P.offsets.assign(n + 1, 0);
@@ -350,7 +351,7 @@ plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_g
    * the replays */
   const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   if(ok && k0) ok = cuda_ok(cudaEventRecordWithFlags(k0, st, evf), "event");
-  if(ok) ok = cuda_ok(launch_workqueue(P.T, tun, &P.wave, P.device, st),
+  if(ok) ok = cuda_ok(launch_workqueue(P.T, tun, P.wave, P.device, st),
                       tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   if(ok && k1) ok = cuda_ok(cudaEventRecordWithFlags(k1, st, evf), "event");
   for(size_t i = 0; ok && !P.accum_out && i < n; ++i) {

@@ -10,7 +10,6 @@ namespace {
 
 struct Workspace {
   DevBuf acc, out, cnt, tables;
-  WaveBufs wave;
   size_t acc_bytes = 0, out_bytes = 0;
 };
 
@@ -80,7 +79,8 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
   } else {
     R.acc = acc;
     R.tacc = tacc;
-    ok = ok && cuda_ok(launch_workqueue_single(scn->d, R, ws.tables.ptr, ws.cnt.ptr, tun, &ws.wave,
+    ok = ok && cuda_ok(launch_workqueue_single(scn->d, R, ws.tables.ptr, ws.cnt.ptr, tun,
+                                               &thread_wave(scn->device),
                                                scn->device, st),
                        tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   }

@@ -96,6 +96,10 @@ struct DScene {
   /* leaf of every cell of every octree, (node index in its tree) << 5 | level:
    * grid `grid_rank[q*3+prop]' of ncell entries; null when it did not fit */
   const uint32_t* leaf_grid;
+  /* or, per cell of every octree, its leaf's kmin/kmax and level (same
+   * ranks); null unless built instead of leaf_grid */
+  const float2* maj_grid;
+  const uint8_t* lvl_grid;
   const uint32_t* grid_rank; /* [nq*3] */
   uint64_t ncell;            /* def[0] * def[1] * def[2] */
   /* ground */

@@ -159,13 +159,12 @@ count_grid(void* cnt, const Path& p)
 
 /* Copy the scene and request tables of a launch into shared memory (one
  * copy per block) and point T at them */
-/* A path held in shared memory.  8 bytes of padding give an odd number of
- * 8-byte words per slot, so a warp's 8-byte accesses to one field of 32
- * slots are free of bank conflicts. */
-struct __align__(8) PathSlot {
-  Path p;
-  uint32_t pad[2];
-};
+/* A path held in shared memory, padded to an odd number of 8-byte words
+ * when the path has an even number, so that a warp's 8-byte accesses to one
+ * field of 32 slots are free of bank conflicts. */
+template <bool Pad> struct __align__(8) PathSlotT { Path p; uint32_t pad[2]; };
+template <> struct __align__(8) PathSlotT<false> { Path p; };
+using PathSlot = PathSlotT<sizeof(Path) % 16 == 0>;
 static_assert(sizeof(PathSlot) % 16 == 8, "odd number of 8-byte words per slot");
 
 /* Shared-memory bytes of the path slots of a block (16-byte rounded) */

@@ -115,9 +115,12 @@ void build_octree(const DScene& hs, const float* lwc, const float* sig3, const f
                   std::vector<uint32_t>& nodes);
 
 /* Leaf of every cell of every built octree (octree_gpu.cu): false when the
- * grids do not fit or cannot be indexed (the traversal then descends) */
+ * grids do not fit or cannot be indexed (the traversal then descends).
+ * `majorants': each cell holds its leaf's kmin/kmax (float2, the ntrees x
+ * ncell array first) and level (u8, after it) instead of node << 5 | level. */
 bool build_leaf_grids(const DScene& S, const std::vector<uint64_t>& tree_base,
-                      const std::vector<uint64_t>& tree_count, DevBuf& grids, std::vector<uint32_t>& rank);
+                      const std::vector<uint64_t>& tree_count, DevBuf& grids, std::vector<uint32_t>& rank,
+                      bool majorants);
 
 /* Ground mesh: validation, BVH and device tables into S (ground.cpp);
  * `upload' copies a host array to a device buffer owned by the scene */
@@ -225,6 +228,12 @@ struct WaveBufs {
 };
 /* Device bytes of one path slot */
 size_t wave_slot_bytes();
+/* Grow-only slot pool of the calling host thread on `device', for the calls
+ * that run the wavefront engine to completion before they return (one call
+ * at a time per thread): a call reuses the slots of the last one instead of
+ * allocating and freeing some 460 MB of device memory and its pinned control
+ * block. */
+WaveBufs& thread_wave(int device);
 cudaError_t launch_wavefront(const PTables& T, const htrdr_gpu_tuning& tun, WaveBufs& B,
                              int device, cudaStream_t st);
 /* Serving pool of P slots driven chunk by chunk (the caller owns the queue):

@@ -170,6 +170,28 @@ k_leafgrid(const uint4* __restrict__ nodes, uint32_t depth, uint32_t nx, uint32_
   grid[c] = (n << 5) | L;
 }
 
+/* Majorants and level of the leaf of every cell of one tree (the same
+ * descent): the trace reads a cell's kmin/kmax and voxel size with two
+ * independent loads instead of the grid entry, then the node */
+__global__ void
+k_majgrid(const uint4* __restrict__ nodes, uint32_t depth, uint32_t nx, uint32_t ny, uint32_t nz,
+          float2* maj, uint8_t* lvl)
+{
+  const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if(c >= (uint64_t)nx * ny * nz) return;
+  const uint32_t x = (uint32_t)(c % nx), y = (uint32_t)((c / nx) % ny), z = (uint32_t)(c / ((uint64_t)nx * ny));
+  uint32_t n = 0, L = depth;
+  uint32_t child = nodes[0].z;
+  while(child != HG_LEAF && L > 0) {
+    --L;
+    n = child + (((x >> L) & 1u) | (((y >> L) & 1u) << 1) | (((z >> L) & 1u) << 2));
+    child = nodes[n].z;
+  }
+  const uint4 v = nodes[n];
+  maj[c] = make_float2(__uint_as_float(v.x), __uint_as_float(v.y));
+  lvl[c] = (uint8_t)L;
+}
+
 }  // namespace
 
 /* Leaf grids of the built trees (tree_count[i] > 0, in index order) into
@@ -178,7 +200,8 @@ k_leafgrid(const uint4* __restrict__ nodes, uint32_t depth, uint32_t nx, uint32_
  * is too large for the 27-bit node index of an entry. */
 bool
 build_leaf_grids(const DScene& S, const std::vector<uint64_t>& tree_base,
-                 const std::vector<uint64_t>& tree_count, DevBuf& grids, std::vector<uint32_t>& rank)
+                 const std::vector<uint64_t>& tree_count, DevBuf& grids, std::vector<uint32_t>& rank,
+                 bool majorants)
 {
   const uint64_t ncell = (uint64_t)S.def[0] * S.def[1] * S.def[2];
   rank.assign(tree_base.size(), 0);
@@ -191,13 +214,21 @@ build_leaf_grids(const DScene& S, const std::vector<uint64_t>& tree_base,
   if(!ntrees || !ncell) return false;
   size_t free_b = 0, total_b = 0;
   if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
-  const uint64_t bytes = (uint64_t)ntrees * ncell * 4;
+  const uint64_t bytes = (uint64_t)ntrees * ncell * (majorants ? 9 : 4);
   if(bytes > free_b / 2) return false;
   if(!grids.alloc(bytes)) return false;
   for(size_t i = 0; i < tree_count.size(); ++i) {
     if(!tree_count[i]) continue;
-    k_leafgrid<<<grid_of(ncell, 256), 256>>>(S.nodes + tree_base[i], S.depth, S.def[0], S.def[1],
-                                              S.def[2], (uint32_t*)grids.ptr + (uint64_t)rank[i] * ncell);
+    const uint64_t off = (uint64_t)rank[i] * ncell;
+    if(majorants) {
+      float2* maj = (float2*)grids.ptr;
+      uint8_t* lvl = (uint8_t*)(maj + (uint64_t)ntrees * ncell);
+      k_majgrid<<<grid_of(ncell, 256), 256>>>(S.nodes + tree_base[i], S.depth, S.def[0], S.def[1],
+                                               S.def[2], maj + off, lvl + off);
+    } else {
+      k_leafgrid<<<grid_of(ncell, 256), 256>>>(S.nodes + tree_base[i], S.depth, S.def[0], S.def[1],
+                                                S.def[2], (uint32_t*)grids.ptr + off);
+    }
   }
   return cuda_ok(cudaGetLastError(), "leaf grids") && cuda_ok(cudaDeviceSynchronize(), "leaf grids");
 }

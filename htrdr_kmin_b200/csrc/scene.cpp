@@ -903,10 +903,27 @@ scene_create(int device, const htrdr_gpu_scene_desc* desc, const char* cache_pat
     S.ncell = (uint64_t)S.def[0] * S.def[1] * S.def[2];
     auto grids = std::make_unique<DevBuf>();
     std::vector<uint32_t> rank;
-    if(HG_LEAF_GRID && build_leaf_grids(S, scn->tree_base, scn->tree_count, *grids, rank)) {
+    /* the majorant grid (9 B per cell and tree) where it fits, else the node
+     * grid (4 B), else none */
+    bool maj = HG_LEAF_GRID == 2, built = false;
+    if(HG_LEAF_GRID) {
+      built = build_leaf_grids(S, scn->tree_base, scn->tree_count, *grids, rank, maj);
+      if(!built && maj) {
+        cudaGetLastError();
+        grids = std::make_unique<DevBuf>();
+        maj = false;
+        built = build_leaf_grids(S, scn->tree_base, scn->tree_count, *grids, rank, false);
+      }
+    }
+    if(built) {
       if(!(S.grid_rank = (const uint32_t*)upload(rank.data(), rank.size() * 4)))
         return HTRDR_GPU_RES_MEM_ERR;
-      S.leaf_grid = (const uint32_t*)grids->ptr;
+      if(maj) {
+        S.maj_grid = (const float2*)grids->ptr;
+        S.lvl_grid = (const uint8_t*)grids->ptr + grids->bytes / 9 * 8;
+      } else {
+        S.leaf_grid = (const uint32_t*)grids->ptr;
+      }
       scn->bytes += grids->bytes;
       scn->bufs.push_back(std::move(grids));
     } else {

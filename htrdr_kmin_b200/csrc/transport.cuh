@@ -477,7 +477,6 @@ struct Path {
   double w, wdirect, inv_pdf, L_sun, weight, wlen_d;
   float ksi, tr_abs, R, refl, sun_ipdf, gdist, g, cosN, wlen;
   uint32_t bounces;
-  int32_t site_cell, site_layer;
   uint32_t pix, ireal, ri;
   /* ground: the hit of the walk's last ground query, and the surface the
    * path leaves (for the self-hit rule) */
@@ -584,9 +583,15 @@ trace_begin(Path& p, const DScene& S, int kind, int prop, float3 o, float3 d, fl
   T.tcur = 0.f;
   T.steps = 0;
   T.region = 0;
-  T.site_cell = -1;
-  T.site_layer = -1;
-  if(kind == TK_TRANS) T.Ts = p.rng.exp1(); /* ..._sw.c:239 */
+  if(kind == TK_TRANS) {
+    /* a transmissivity trace sets no collision site: the site of the free
+     * path before it stays for the scattering that follows (the absorption
+     * transmissivity to a collision site, ..._sw.c:394-398) */
+    T.Ts = p.rng.exp1(); /* ..._sw.c:239 */
+  } else {
+    T.site_cell = -1;
+    T.site_layer = -1;
+  }
   p.state = ST_TRACE;
   p.ret = ret;
 
@@ -607,7 +612,7 @@ trace_begin(Path& p, const DScene& S, int kind, int prop, float3 o, float3 d, fl
       T.cb0 = c0;
       T.cb1 = c1;
       T.base = S.tree_base[(size_t)p.q * 3 + prop];
-      T.grank = S.leaf_grid ? __ldg(S.grid_rank + (size_t)p.q * 3 + prop) : 0u;
+      T.grank = S.grid_rank ? __ldg(S.grid_rank + (size_t)p.q * 3 + prop) : 0u;
     }
   }
   region_enter(T, S);
@@ -698,6 +703,21 @@ trace_finish(Path& p, bool hit)
 {
   p.tr.hit = hit ? 1 : 0;
   p.state = p.ret;
+}
+
+/* SW walk after a free path that ended by a collision in the medium: the
+ * absorption transmissivity along that free path, from its origin to the
+ * collision site (..._sw.c:385-398).  It reads and writes only the trace
+ * part of the path, so the wavefront's trace stage runs it in place of an
+ * event-stage visit.  Returns the collision site (pos_next). */
+__device__ __forceinline__ float3
+sw_scat_volume(Path& p, const DScene& S)
+{
+  const float3 o = p.tr.o, d = p.tr.d;
+  const float tdst = p.tr.tcur;
+  p.flags &= ~(PF_SURFACE | PF_PREV_GROUND);
+  trace_begin(p, S, TK_TRANS, HG_KA, o, d, 0.f, tdst, ST_SW_ABS_END);
+  return madd3(o, d, tdst);
 }
 
 /* Vertical optical depth from z = 0 to z (clamped to the column) */
@@ -828,7 +848,18 @@ trace_step(Path& p, const DScene& S)
   uint4 v;
   bool leaf_root = false;
   bool found = false;
-  if(T.start == 1) {
+  if(S.maj_grid) {
+    /* the leaf's majorants and level from the cell: two independent loads,
+     * no node read */
+    const uint64_t gi = (uint64_t)T.grank * S.ncell
+                      + ((uint64_t)T.c[2] * S.def[1] + T.c[1]) * S.def[0] + T.c[0];
+    const float2 mm = __ldg(S.maj_grid + gi);
+    L = __ldg(S.lvl_grid + gi);
+    ++p.c_grid;
+    v.x = __float_as_uint(mm.x);
+    v.y = __float_as_uint(mm.y);
+    found = true;
+  } else if(T.start == 1) {
     base = T.p_base; L = T.p_level;
   } else if(S.leaf_grid) {
     /* the leaf from the cell's grid entry: two dependent loads whatever the
@@ -1271,20 +1302,14 @@ path_event(Path& p, const DScene& S, const DRequest& R)
       }
 
       case ST_SW_SCAT_END: if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; } else {
-        const bool svx = p.tr.hit != 0;
-        if(p.gdist < 0.f && !svx) { p.state = ST_RAD_END; break; }
-        const bool surface = !svx;
-        const float tdst = surface ? p.gdist : p.tr.tcur;
+        if(p.tr.hit) { p.pnext = sw_scat_volume(p, S); return; } /* the trace origin is p.pos */
+        if(p.gdist < 0.f) { p.state = ST_RAD_END; break; }
+        /* the ground: scattering at the surface */
+        const float tdst = p.gdist;
         p.pnext = madd3(p.pos, p.dir, tdst);
-        if(surface) {
-          p.flags |= PF_SURFACE | PF_PREV_GROUND;
-          p.prev_prim = p.gprim;
-          p.prev_edge = p.gedge;
-        } else {
-          p.flags &= ~(PF_SURFACE | PF_PREV_GROUND);
-        }
-        p.site_cell = p.tr.site_cell;
-        p.site_layer = p.tr.site_layer;
+        p.flags |= PF_SURFACE | PF_PREV_GROUND;
+        p.prev_prim = p.gprim;
+        p.prev_edge = p.gedge;
         trace_begin(p, S, TK_TRANS, HG_KA, p.pos, p.dir, 0.f, tdst, ST_SW_ABS_END);
         return;
       }
@@ -1292,8 +1317,9 @@ path_event(Path& p, const DScene& S, const DRequest& R)
       case ST_SW_ABS_END: if constexpr(!(V & HV_SW)) { path_variant_miss(p); break; } else {
         p.tr_abs = p.tr.hit ? 0.f : (float)(p.tr.Tmin != 0.0 ? exp(-p.tr.Tmin) : 1.0);
         if(p.tr_abs <= 0.f) { p.state = ST_RAD_END; break; }
-        const ScatOut so = sw_scatter<V>(S, p.rng, p.dir, p.g, p.flags, p.refl, p.site_cell,
-                                      p.site_layer, p.band, p.q, p.gprim, p.gN, p.wlen_d);
+        /* the collision site of the free path: the absorption trace keeps it */
+        const ScatOut so = sw_scatter<V>(S, p.rng, p.dir, p.g, p.flags, p.refl, p.tr.site_cell,
+                                      p.tr.site_layer, p.band, p.q, p.gprim, p.gN, p.wlen_d);
         p.rng = so.rng;
         p.flags = so.flags;
         p.dnext = so.dnext;

@@ -28,6 +28,8 @@
 #include "engine.cuh"
 
 #include <algorithm>
+#include <map>
+#include <memory>
 #include <cstring>
 
 namespace hg {
@@ -37,6 +39,12 @@ namespace {
 constexpr uint32_t kPathV4 = (uint32_t)((sizeof(Path) + 15) / 16);
 constexpr uint32_t kTraceV4 = (uint32_t)((offsetof(Path, org) + 15) / 16);
 static_assert(kTraceV4 <= kPathV4, "trace part inside the path");
+/* The vector holding the collision site of a SW free path (pnext), which the
+ * trace stage writes when it runs the absorption trace itself.  Its last
+ * word is dnext.x, dead from there until ST_SW_ABS_END sets dnext. */
+constexpr uint32_t kPnextV4 = (uint32_t)(offsetof(Path, pnext) / 16);
+static_assert(offsetof(Path, pnext) % 16 == 0 && offsetof(Path, dnext) == offsetof(Path, pnext) + 12,
+              "pnext and dnext.x fill one 16-byte vector");
 
 /* Slot storage: a path is kPathV4 16-byte vectors.  HG_WAVE_SOA 0 (default)
  * keeps a slot's vectors contiguous (a lane reading its own slot uses every
@@ -247,6 +255,13 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
     if(!__any_sync(0xffffffffu, have)) break;
     if(have) {
       trace_step<HV_ALL>(p, T.scenes[p.si]);
+      if(p.state == ST_SW_SCAT_END && p.tr.hit) {
+        /* a SW free path ended in the medium: its absorption trace runs
+         * here, without a round trip through the event stage */
+        const float3 pn = sw_scat_volume(p, T.scenes[p.si]);
+        W.paths[vec_at(s, kPnextV4, W.P)] =
+          make_uint4(__float_as_uint(pn.x), __float_as_uint(pn.y), __float_as_uint(pn.z), 0u);
+      }
       if(p.state != ST_TRACE || --left == 0) {
         p.t0 = gtimer() - p.t0;
         store_trace(p, W.paths, s, W.P);
@@ -417,6 +432,15 @@ WaveBufs::~WaveBufs()
   if(host_ctl) cudaFreeHost(host_ctl);
   if(ev[0]) cudaEventDestroy(ev[0]);
   if(ev[1]) cudaEventDestroy(ev[1]);
+}
+
+WaveBufs&
+thread_wave(int device)
+{
+  static thread_local std::map<int, std::unique_ptr<WaveBufs>> pools;
+  std::unique_ptr<WaveBufs>& w = pools[device];
+  if(!w) w = std::make_unique<WaveBufs>();
+  return *w;
 }
 
 /* Slots of a run: enough paths in flight to keep every trace lane busy
