@@ -561,10 +561,11 @@ def run_serve(args):
 
 def alg_bytes_of(st) -> int:
     """Algorithmic bytes of a launch from its counters: 16 per majorant node
-    fetched, 4 per leaf-grid entry read, 8 per tentative collision (its
-    raw-property gather: cloud cell and gas layer) and 32 per realisation (the
-    read-modify-write of its FP64 sums and count)."""
-    return 16 * st.nodes + 4 * st.grid_lookups + 8 * st.collisions + 32 * st.realisations
+    fetched, the leaf-grid bytes read (9 per majorant-grid lookup, 4 per
+    node-grid lookup), 8 per tentative collision (its raw-property gather:
+    cloud cell and gas layer) and 32 per realisation (the read-modify-write
+    of its FP64 sums and count)."""
+    return 16 * st.nodes + st.grid_bytes + 8 * st.collisions + 32 * st.realisations
 
 
 def traffic_per_launch(kernel: str, alg_bytes: int):
@@ -811,7 +812,7 @@ def measure(args, api, su: "Setup", desc: str, tuning, tuning_src: str, rank: in
         "batched_vs_plain": plain_ms / kms,
         "segments_per_s": last.segments / (kms * 1e-3),
         "counters": {"segments": last.segments, "nodes": last.nodes,
-                     "grid_lookups": last.grid_lookups, "collisions": last.collisions,
+                     "grid_bytes": last.grid_bytes, "collisions": last.collisions,
                      "realisations": last.realisations, "failures": last.failures},
     }
     if sampler:
@@ -890,7 +891,7 @@ def main():
         print(json.dumps({"workload": desc, "tuning": tuning_dict(tuning, "command line"),
                           "kernel_ms": st.kernel_ms, "launches": st.launches, "alg_bytes": alg,
                           "counters": {"segments": st.segments, "nodes": st.nodes,
-                                       "grid_lookups": st.grid_lookups,
+                                       "grid_bytes": st.grid_bytes,
                                        "collisions": st.collisions, "realisations": st.realisations}}),
               flush=True)
         su.close()

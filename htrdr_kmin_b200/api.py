@@ -105,7 +105,7 @@ class Stats(C.Structure):
     _fields_ = [("realisations", C.c_uint64), ("segments", C.c_uint64), ("nodes", C.c_uint64),
                 ("collisions", C.c_uint64), ("failures", C.c_uint64),
                 ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("launches", C.c_uint64),
-                ("grid_lookups", C.c_uint64)]
+                ("grid_bytes", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

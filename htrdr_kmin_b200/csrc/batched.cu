@@ -25,6 +25,8 @@
 #include "engine.cuh"
 
 #include <algorithm>
+#include <map>
+#include <memory>
 #include <cstring>
 
 namespace hg {
@@ -243,6 +245,38 @@ persistent_capacity(uint32_t block_size, uint32_t blocks_per_sm, int device)
   return (uint64_t)std::max(per_sm, 1) * (uint64_t)nsm * block_size;
 }
 
+/* Device buffers of a plan: tables, accumulators, counters, output staging */
+struct PlanBufs {
+  DevBuf d_scenes, d_reqs, d_items, d_offsets, d_acc, d_cnt, d_out;
+};
+
+/* Grow-only buffers of the one-shot calls of a host thread on a device (one
+ * call at a time per thread): a call reuses those of the last one, as
+ * freeing device memory after every call cost up to 0.6 s of host time */
+PlanBufs&
+thread_plan_bufs(int device)
+{
+  static thread_local std::map<int, std::unique_ptr<PlanBufs>> bufs;
+  std::unique_ptr<PlanBufs>& b = bufs[device];
+  if(!b) b = std::make_unique<PlanBufs>();
+  return *b;
+}
+
+/* `b' holding at least `n' bytes (its contents are not kept) */
+bool
+reserve(DevBuf& b, size_t n)
+{
+  if(b.ptr && b.bytes >= n) return true;
+  if(b.ptr) { cudaFree(b.ptr); b.ptr = nullptr; b.bytes = 0; }
+  return b.alloc(n);
+}
+
+bool
+fill(DevBuf& b, const void* src, size_t n)
+{
+  return reserve(b, n) && (!n || cuda_ok(cudaMemcpy(b.ptr, src, n, cudaMemcpyHostToDevice), "cudaMemcpy H2D"));
+}
+
 /* Device state of a set of items: tables, accumulators, counters */
 struct Plan {
   int device = 0;
@@ -251,7 +285,8 @@ struct Plan {
   std::vector<PItem> items;
   std::vector<uint64_t> offsets;
   std::vector<size_t> out_off;
-  DevBuf d_scenes, d_reqs, d_items, d_offsets, d_acc, d_cnt, d_out;
+  PlanBufs own;           /* a reusable batch's buffers (its graph holds their addresses) */
+  PlanBufs* B = &own;     /* the buffers in use: `own', or the thread's for a one-shot call */
   size_t acc_bytes = 0;
   bool accum_out = false; /* the items' buffers receive the accumulators */
   std::vector<size_t> item_acc_bytes;
@@ -261,7 +296,7 @@ struct Plan {
 
 static htrdr_gpu_res_T
 plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out,
-           bool accum_out = false)
+           bool accum_out = false, bool one_shot = true)
 {
   const int device = items[0].scene ? items[0].scene->device : -1;
   for(size_t i = 0; i < n; ++i) {
@@ -276,6 +311,8 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out,
   if(!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return HTRDR_GPU_RES_BAD_OP;
   P.device = device;
   P.wave = &thread_wave(device);
+  if(one_shot) P.B = &thread_plan_bufs(device);
+  PlanBufs& B = *P.B;
   P.reqs.resize(n);
   P.items.resize(n);
   P.offsets.assign(n + 1, 0);
@@ -306,33 +343,33 @@ plan_build(Plan& P, const htrdr_gpu_batch_item* items, size_t n, bool host_out,
     if(host_out) out_bytes += (items[i].layout.pitch * items[i].layout.height + 255) & ~(size_t)255;
   }
   P.acc_bytes = accum_out ? 0 : acc_total * sizeof(DAccum);
-  if((!accum_out && !P.d_acc.alloc(P.acc_bytes)) || !P.d_cnt.alloc(128) || !P.d_out.alloc(out_bytes))
+  if((!accum_out && !reserve(B.d_acc, P.acc_bytes)) || !reserve(B.d_cnt, 128) || !reserve(B.d_out, out_bytes))
     return HTRDR_GPU_RES_MEM_ERR;
   P.item_acc_bytes.assign(n, 0);
   for(size_t i = 0; i < n; ++i) {
     const uint64_t npix = (uint64_t)P.reqs[i].width * P.reqs[i].height;
     const uint32_t nch = P.reqs[i].mode == HG_IMAGE_CIE ? 3u : 1u;
-    P.reqs[i].acc = accum_out ? (DAccum*)items[i].buffer : (DAccum*)P.d_acc.ptr + acc_off[i];
+    P.reqs[i].acc = accum_out ? (DAccum*)items[i].buffer : (DAccum*)B.d_acc.ptr + acc_off[i];
     P.reqs[i].tacc = P.reqs[i].acc + npix * nch;
     P.item_acc_bytes[i] = npix * (nch + 1) * sizeof(DAccum);
   }
-  if(!P.d_scenes.upload(P.scenes.data(), P.scenes.size() * sizeof(DScene))
-  || !P.d_reqs.upload(P.reqs.data(), n * sizeof(DRequest))
-  || !P.d_items.upload(P.items.data(), n * sizeof(PItem))
-  || !P.d_offsets.upload(P.offsets.data(), (n + 1) * 8))
+  if(!fill(B.d_scenes, P.scenes.data(), P.scenes.size() * sizeof(DScene))
+  || !fill(B.d_reqs, P.reqs.data(), n * sizeof(DRequest))
+  || !fill(B.d_items, P.items.data(), n * sizeof(PItem))
+  || !fill(B.d_offsets, P.offsets.data(), (n + 1) * 8))
     return HTRDR_GPU_RES_MEM_ERR;
   PTables& T = P.T;
-  T.scenes = (const DScene*)P.d_scenes.ptr;
-  T.reqs = (const DRequest*)P.d_reqs.ptr;
-  T.items = (const PItem*)P.d_items.ptr;
-  T.offsets = (const uint64_t*)P.d_offsets.ptr;
+  T.scenes = (const DScene*)B.d_scenes.ptr;
+  T.reqs = (const DRequest*)B.d_reqs.ptr;
+  T.items = (const PItem*)B.d_items.ptr;
+  T.offsets = (const uint64_t*)B.d_offsets.ptr;
   T.nscenes = (uint32_t)P.scenes.size();
   T.variant = tables_variant(P.scenes, P.reqs);
   T.nreqs = (uint32_t)n;
   T.nitems = (uint32_t)n;
   T.total = P.offsets[n];
-  T.cnt = P.d_cnt.ptr;
-  T.next = (unsigned long long*)((char*)P.d_cnt.ptr + 64);
+  T.cnt = B.d_cnt.ptr;
+  T.next = (unsigned long long*)((char*)B.d_cnt.ptr + 64);
   return HTRDR_GPU_RES_OK;
 }
 
@@ -342,9 +379,9 @@ static bool
 plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning& tun,
              bool host_out, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1, bool capturing = false)
 {
-  bool ok = cuda_ok(cudaMemsetAsync(P.d_cnt.ptr, 0, 128, st), "memset");
+  bool ok = cuda_ok(cudaMemsetAsync(P.B->d_cnt.ptr, 0, 128, st), "memset");
   if(!P.accum_out)
-    ok = ok && cuda_ok(cudaMemsetAsync(P.d_acc.ptr, 0, P.acc_bytes, st), "memset");
+    ok = ok && cuda_ok(cudaMemsetAsync(P.B->d_acc.ptr, 0, P.acc_bytes, st), "memset");
   for(size_t i = 0; ok && P.accum_out && i < n; ++i)
     ok = cuda_ok(cudaMemsetAsync(P.reqs[i].acc, 0, P.item_acc_bytes[i], st), "memset");
   /* inside a stream capture an event record must be an external node to time
@@ -355,7 +392,7 @@ plan_enqueue(Plan& P, const htrdr_gpu_batch_item* items, size_t n, const htrdr_g
                       tun.engine == HTRDR_GPU_ENGINE_WAVEFRONT ? "wavefront" : "k_persistent");
   if(ok && k1) ok = cuda_ok(cudaEventRecordWithFlags(k1, st, evf), "event");
   for(size_t i = 0; ok && !P.accum_out && i < n; ++i) {
-    char* dout = host_out ? (char*)P.d_out.ptr + P.out_off[i] : (char*)items[i].buffer;
+    char* dout = host_out ? (char*)P.B->d_out.ptr + P.out_off[i] : (char*)items[i].buffer;
     ok = cuda_ok(launch_finalize(P.reqs[i], P.reqs[i].acc, P.reqs[i].tacc, dout,
                                  items[i].layout.pitch, st), "k_finalize");
     if(ok && host_out)
@@ -371,7 +408,7 @@ read_stats(const unsigned long long c[6], float kms, float tms, uint64_t launche
 {
   if(!stats) return;
   stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
-  stats->realisations = c[3]; stats->failures = c[4]; stats->grid_lookups = c[5];
+  stats->realisations = c[3]; stats->failures = c[4]; stats->grid_bytes = c[5];
   stats->kernel_ms = kms; stats->total_ms = tms;
   stats->launches = launches;
 }
@@ -455,7 +492,7 @@ batched_impl(htrdr_gpu_batch_item* items, size_t n, const htrdr_gpu_tuning* tuni
   bool ok = plan_enqueue(P, items, n, tun, host, st, e1, e2);
   cudaEventRecord(e3, st);
   unsigned long long c[6] = {0, 0, 0, 0, 0, 0};
-  if(ok) ok = cuda_ok(cudaMemcpyAsync(c, P.d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H");
+  if(ok) ok = cuda_ok(cudaMemcpyAsync(c, P.B->d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, st), "D2H");
   if(ok) ok = cuda_ok(cudaStreamSynchronize(st), "sync");
   if(ok) {
     float k = 0, t = 0;
@@ -586,7 +623,7 @@ try {
   }
   auto b = new htrdr_gpu_batch();
   b->items.assign(items, items + n);
-  htrdr_gpu_res_T res = plan_build(b->plan, b->items.data(), n, false);
+  htrdr_gpu_res_T res = plan_build(b->plan, b->items.data(), n, false, false, false);
   if(res != HTRDR_GPU_RES_OK) { htrdr_gpu_batch_release(b); return res; }
   bool ok = cuda_ok(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream")
          && cuda_ok(cudaEventCreate(&b->e0), "event") && cuda_ok(cudaEventCreate(&b->e1), "event")
@@ -614,7 +651,7 @@ try {
   bool ok = cuda_ok(cudaEventRecord(b->e0, b->stream), "event")
          && cuda_ok(cudaGraphLaunch(b->exec, b->stream), "graph launch")
          && cuda_ok(cudaEventRecord(b->e3, b->stream), "event")
-         && cuda_ok(cudaMemcpyAsync(c, b->plan.d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, b->stream), "D2H")
+         && cuda_ok(cudaMemcpyAsync(c, b->plan.B->d_cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, b->stream), "D2H")
          && cuda_ok(cudaStreamSynchronize(b->stream), "sync");
   if(!ok) return HTRDR_GPU_RES_UNKNOWN_ERR;
   float k = 0, t = 0;

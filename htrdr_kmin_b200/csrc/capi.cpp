@@ -98,7 +98,7 @@ draw_map_impl(htrdr_gpu_scene* scn, const htrdr_gpu_request* req,
     cudaEventElapsedTime(&k, e1, e2);
     cudaEventElapsedTime(&t, e0, e3);
     stats->segments = c[0]; stats->nodes = c[1]; stats->collisions = c[2];
-    stats->realisations = c[3]; stats->failures = c[4]; stats->grid_lookups = c[5];
+    stats->realisations = c[3]; stats->failures = c[4]; stats->grid_bytes = c[5];
     stats->kernel_ms = k; stats->total_ms = t;
     stats->launches = take_launches();
   }

@@ -149,7 +149,7 @@ flush_counts(void* cnt, unsigned long long seg, unsigned long long node, unsigne
   }
 }
 
-/* Leaf-grid lookups of a completed path, added to the launch's total: one
+/* Leaf-grid bytes read by a completed path, added to the launch's total: one
  * atomic per realisation, so that no engine keeps another running counter */
 __device__ __forceinline__ void
 count_grid(void* cnt, const Path& p)

@@ -21,7 +21,7 @@
 
 /* Leaf grids of the octrees (1: built when they fit; 0: never) */
 #ifndef HG_LEAF_GRID
-#define HG_LEAF_GRID 1
+#define HG_LEAF_GRID 2
 #endif
 
 namespace hg {

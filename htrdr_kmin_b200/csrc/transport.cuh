@@ -463,7 +463,7 @@ struct Path {
    * that the wavefront engine's trace stage moves only this prefix of a
    * stored path (HG_TRACE_WORDS). */
   Rng rng;
-  uint32_t c_grid;      /* local counter of leaf-grid lookups (the word before
+  uint32_t c_grid;      /* local counter of leaf-grid bytes read (the word before
                          * the 8-byte aligned Trace: no extra storage) */
   Trace tr;
   uint32_t band, q, flags;
@@ -471,13 +471,17 @@ struct Path {
   unsigned long long t0;
   uint32_t c_seg, c_node, c_tc; /* local counters */
   uint8_t state, ret, mode, chan;
+  /* walk fields the wavefront's trace stage reads or writes when it runs a
+   * LW scattering itself, and the realisation's pixel and index */
+  uint32_t bounces;
+  float gdist;          /* ground distance along the current free path, < 0: none */
+  uint32_t pix, ireal;
   /* event part */
   float3 org, rdir;     /* sensor ray */
   float3 pos, dir, pnext, dnext, sdir;
   double w, wdirect, inv_pdf, L_sun, weight, wlen_d;
-  float ksi, tr_abs, R, refl, sun_ipdf, gdist, g, cosN, wlen;
-  uint32_t bounces;
-  uint32_t pix, ireal, ri;
+  float ksi, tr_abs, R, refl, sun_ipdf, g, cosN, wlen;
+  uint32_t ri;
   /* ground: the hit of the walk's last ground query, and the surface the
    * path leaves (for the self-hit rule) */
   float3 gN;
@@ -488,7 +492,7 @@ struct Path {
 /* 32-bit words of a stored path, and of its trace part */
 #define HG_PATH_WORDS ((uint32_t)(sizeof(Path) / 4))
 #define HG_TRACE_WORDS ((uint32_t)(offsetof(Path, org) / 4))
-static_assert(offsetof(Path, tr) == 40 && offsetof(Path, org) == 224, "trace prefix of 56 words");
+static_assert(offsetof(Path, tr) == 40 && offsetof(Path, org) == 240, "trace prefix of 15 vectors");
 static_assert(sizeof(Path) % 4 == 0 && offsetof(Path, org) % 4 == 0, "word-wise path storage");
 
 __device__ __forceinline__ unsigned long long
@@ -855,7 +859,7 @@ trace_step(Path& p, const DScene& S)
                       + ((uint64_t)T.c[2] * S.def[1] + T.c[1]) * S.def[0] + T.c[0];
     const float2 mm = __ldg(S.maj_grid + gi);
     L = __ldg(S.lvl_grid + gi);
-    ++p.c_grid;
+    p.c_grid += 9;
     v.x = __float_as_uint(mm.x);
     v.y = __float_as_uint(mm.y);
     found = true;
@@ -870,7 +874,7 @@ trace_step(Path& p, const DScene& S)
     L = e & 31u;
     v = __ldg(nodes + n);
     ++p.c_node;
-    ++p.c_grid;
+    p.c_grid += 4;
     found = true;
     if(L < S.depth) {
       const uint32_t oct = ((T.c[0] >> L) & 1u) | (((T.c[1] >> L) & 1u) << 1) | (((T.c[2] >> L) & 1u) << 2);
@@ -1239,6 +1243,38 @@ path_variant_miss(Path& p)
  * is done (ST_DONE) or idle.  V: the kernel variant (HV_* bits); the states
  * of a spectral kind it leaves out and, without HV_MESH, the mesh queries
  * are compiled out. */
+/* Whether the ground of the scene is the plane (its hit record is then the
+ * same at every query: no primitive, no edge, normal +z) */
+template <unsigned V>
+__device__ __forceinline__ bool
+lw_plane_ground(const DScene& S)
+{
+  return !(V & HV_MESH) || !S.g_ntris;
+}
+
+/* LW walk after a scattering in the medium, over a plane ground: the new
+ * direction from the phase function (..._lw.c:235) and the next free path
+ * from the collision site, the head of the walk (..._lw.c:184-205) -- the
+ * steps ST_LW_END and ST_LW_WALK take there.  It reads and writes the trace
+ * part of the path only (the plane's hit record, set at the walk's first
+ * ground query, stays the same) and returns the walk's new position and
+ * direction, which the wavefront's trace stage stores into p.pos / p.dir:
+ * the stage runs it without an event-stage visit.  The caller checks that
+ * the bounce limit is not reached. */
+__device__ __forceinline__ void
+lw_scatter_plane(Path& p, const DScene& S, float3& pos, float3& dir)
+{
+  pos = madd3(p.tr.o, p.tr.d, p.tr.tcur);
+  const float g = __ldg(S.optics + p.band).w;
+  const float u1 = p.rng.uf(), u2 = p.rng.uf();
+  dir = around(p.tr.d, hg_mu(g, u1), u2);
+  p.flags &= ~PF_PREV_GROUND;
+  ++p.bounces;
+  p.gdist = ground_trace(S, pos, dir, 0.f, FLT_MAX, false);
+  p.tr.Ts = p.rng.exp1();
+  trace_begin(p, S, TK_LW, HG_KEXT, pos, dir, 0.f, p.gdist >= 0.f ? p.gdist : FLT_MAX, ST_LW_END);
+}
+
 template <unsigned V>
 __device__ __forceinline__ void
 path_event(Path& p, const DScene& S, const DRequest& R)
@@ -1370,6 +1406,9 @@ path_event(Path& p, const DScene& S, const DRequest& R)
       }
 
       case ST_LW_END: if constexpr(!(V & HV_LW)) { path_variant_miss(p); break; } else {
+        /* the free path just traced started at p.tr.o along p.tr.d (the
+         * walk's position and direction, which the trace stage may have
+         * moved past p.pos / p.dir) */
         const bool svx = p.tr.hit != 0;
         const double wlen_m = p.wlen_d * 1e-9;
         if(p.gdist < 0.f && !svx) { p.w = 0.0; p.state = ST_RAD_END; break; }

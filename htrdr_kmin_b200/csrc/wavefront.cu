@@ -45,6 +45,12 @@ static_assert(kTraceV4 <= kPathV4, "trace part inside the path");
 constexpr uint32_t kPnextV4 = (uint32_t)(offsetof(Path, pnext) / 16);
 static_assert(offsetof(Path, pnext) % 16 == 0 && offsetof(Path, dnext) == offsetof(Path, pnext) + 12,
               "pnext and dnext.x fill one 16-byte vector");
+/* The vectors of the walk's position and direction, which the trace stage
+ * writes when it runs a LW scattering itself: pos.x, pos.y end the first,
+ * pos.z and dir fill the second */
+constexpr uint32_t kPosV4 = (uint32_t)(offsetof(Path, pos) / 16);
+static_assert(offsetof(Path, pos) % 16 == 8 && offsetof(Path, dir) == offsetof(Path, pos) + 12
+              && offsetof(Path, dir) + 12 == (kPosV4 + 2) * 16, "pos and dir end two 16-byte vectors");
 
 /* Slot storage: a path is kPathV4 16-byte vectors.  HG_WAVE_SOA 0 (default)
  * keeps a slot's vectors contiguous (a lane reading its own slot uses every
@@ -261,6 +267,16 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
         const float3 pn = sw_scat_volume(p, T.scenes[p.si]);
         W.paths[vec_at(s, kPnextV4, W.P)] =
           make_uint4(__float_as_uint(pn.x), __float_as_uint(pn.y), __float_as_uint(pn.z), 0u);
+      } else if(p.state == ST_LW_END && p.tr.hit && p.tr.event == 1 && p.bounces < HG_MAX_BOUNCES
+             && lw_plane_ground<HV_ALL>(T.scenes[p.si])) {
+        /* a LW scattering in the medium: the walk goes on here */
+        float3 pos, dir;
+        lw_scatter_plane(p, T.scenes[p.si], pos, dir);
+        uint4* v = W.paths + vec_at(s, kPosV4, W.P);
+        ((uint2*)v)[1] = make_uint2(__float_as_uint(pos.x), __float_as_uint(pos.y));
+        v = W.paths + vec_at(s, kPosV4 + 1, W.P);
+        *v = make_uint4(__float_as_uint(pos.z), __float_as_uint(dir.x), __float_as_uint(dir.y),
+                        __float_as_uint(dir.z));
       }
       if(p.state != ST_TRACE || --left == 0) {
         p.t0 = gtimer() - p.t0;

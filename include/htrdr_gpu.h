@@ -141,8 +141,9 @@ struct htrdr_gpu_stats {
   double kernel_ms;      /* CUDA-event time of the transport kernel(s) */
   double total_ms;       /* whole call, device side */
   uint64_t launches;     /* kernels the call launched (transport, initialisation, finalize) */
-  uint64_t grid_lookups; /* leaf-grid entries read (4 bytes each; every one is
-                          * followed by one of the `nodes' fetches) */
+  uint64_t grid_bytes;   /* bytes of leaf-grid entries read: 9 per majorant-grid
+                          * lookup (a leaf's kmin/kmax and level, no node
+                          * fetch), 4 per node-grid lookup (then a node) */
 };
 
 struct htrdr_gpu_scene;

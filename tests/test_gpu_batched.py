@@ -71,7 +71,7 @@ def test_wavefront_equals_plain(gpu_lib, slots, budget, bs, tail):
     ref, sref = gpu_lib.draw_maps_batched(items, gpu_lib.default_tuning())
     assert st["realisations"] == sref["realisations"]
     assert st["segments"] == sref["segments"] and st["collisions"] == sref["collisions"]
-    assert st["nodes"] == sref["nodes"] and st["grid_lookups"] == sref["grid_lookups"]
+    assert st["nodes"] == sref["nodes"] and st["grid_bytes"] == sref["grid_bytes"]
     for (gs, req), b, r in zip(items, bufs, ref):
         gs.set_engine(gpu_lib.ENGINE_PLAIN)
         p, _ = gs.draw_map(req)
@@ -120,11 +120,10 @@ def test_draw_map_engines_agree(gpu_lib):
         _cmp(wave, plain, req.mode)
         assert sw["segments"] == sp["segments"]
         # every path takes the same voxel steps on every engine, so it reads
-        # the same leaf-grid entries, each followed by one node fetch
-        assert sp["grid_lookups"] == spp["grid_lookups"] == sw["grid_lookups"]
+        # the same leaf-grid entries and majorant nodes
+        assert sp["grid_bytes"] == spp["grid_bytes"] == sw["grid_bytes"]
         assert sp["nodes"] == spp["nodes"] == sw["nodes"]
-        assert sp["grid_lookups"] <= sp["nodes"]
-        lookups += sp["grid_lookups"]
+        lookups += sp["grid_bytes"]
         t.trace_budget, t.wave_slots, t.wave_tail = 5, 333, 100
         gs.set_engine(gpu_lib.ENGINE_WAVEFRONT, t)
         wave2, _ = gs.draw_map(req)
