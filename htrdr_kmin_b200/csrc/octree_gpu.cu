@@ -243,6 +243,10 @@ struct Worker {
   ~Worker() { if(st) cudaStreamDestroy(st); }
 };
 
+#ifndef HG_BUILD_WORKERS
+#define HG_BUILD_WORKERS 8
+#endif
+
 /* Builds the trees of `tasks' ((quad, property) pairs) on the device into one
  * pool; tree_base/tree_count are filled per task index.  The trees are
  * shared among up to 8 workers, each a host thread with its own stream and
@@ -282,7 +286,7 @@ build_octrees_gpu(const DScene& S, const float* d_lwc, const int2* d_cl, const f
   size_t free_b = 0, total_b = 0;
   if(!cuda_ok(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo")) return false;
   const size_t budget = std::min<size_t>(free_b / 4, (size_t)16 << 30);
-  const size_t nw = std::max<size_t>(1, std::min<size_t>({(size_t)8, tasks.size(),
+  const size_t nw = std::max<size_t>(1, std::min<size_t>({(size_t)HG_BUILD_WORKERS, tasks.size(),
                                                            budget / std::max<size_t>(per_worker, 1)}));
   std::vector<std::unique_ptr<Worker>> workers;
   for(size_t w = 0; w < nw; ++w) {

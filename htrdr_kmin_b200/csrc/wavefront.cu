@@ -52,6 +52,38 @@ constexpr uint32_t kPosV4 = (uint32_t)(offsetof(Path, pos) / 16);
 static_assert(offsetof(Path, pos) % 16 == 8 && offsetof(Path, dir) == offsetof(Path, pos) + 12
               && offsetof(Path, dir) + 12 == (kPosV4 + 2) * 16, "pos and dir end two 16-byte vectors");
 
+/* Gas-region batching of the trace stage (0: off).  Measured on a B200
+ * (Mrealisations/s, off / batch 4 wait 8 / batch 8 wait 16): full-size mix
+ * 1.876 / 1.977 / 1.973, 1/4-scale mix 3.01 / 3.22 / 3.28, SW image 12.0 /
+ * 12.1 / 12.3, LW flux 227 / 230 / 227. */
+#ifndef HG_GAS_BATCH
+#define HG_GAS_BATCH 8
+#endif
+#ifndef HG_GAS_WAIT
+#define HG_GAS_WAIT 16
+#endif
+/* Batching of the trace stage's path loads (0: off).  Measured (off /
+ * batch 4 wait 8 / batch 8 wait 16, gas batching on): full-size mix 1.979 /
+ * 1.966 / 1.972, 1/4-scale mix 3.28 / 3.36 / 3.43, SW image 12.26 / 12.45 /
+ * 12.59, LW flux 225 / 225 / 232 Mrealisations/s. */
+#ifndef HG_FETCH_BATCH
+#define HG_FETCH_BATCH 8
+#endif
+#ifndef HG_FETCH_WAIT
+#define HG_FETCH_WAIT 16
+#endif
+
+/* Whether the next step of a trace is a whole gas region (the analytic
+ * column of gas_region) */
+__device__ __forceinline__ bool
+trace_in_gas(const Trace& T)
+{
+  const int nreg = T.has_cloud ? 3 : 1;
+  if(T.region >= nreg) return false;
+  const bool cloud = T.has_cloud && T.region == 1;
+  return !cloud && T.d.z != 0.f;
+}
+
 /* Slot storage: a path is kPathV4 16-byte vectors.  HG_WAVE_SOA 0 (default)
  * keeps a slot's vectors contiguous (a lane reading its own slot uses every
  * byte of the sectors it touches, whatever slots its warp holds); 1 stores
@@ -109,6 +141,36 @@ store_trace(const Path& p, uint4* paths, uint32_t s, uint32_t P)
   memcpy(v, &p, kTraceV4 * 16);
 #pragma unroll
   for(uint32_t i = 0; i < kTraceV4; ++i) paths[vec_at(s, i, P)] = v[i];
+}
+
+/* Whether a trace that just ended leads to a transition the trace stage runs
+ * itself: the absorption trace after a SW collision in the medium, the next
+ * free path after a LW scattering in the medium over a plane ground */
+__device__ __forceinline__ bool
+transition_here(const Path& p, const DScene& S)
+{
+  if(p.state == ST_SW_SCAT_END) return p.tr.hit != 0;
+  return p.state == ST_LW_END && p.tr.hit && p.tr.event == 1 && p.bounces < HG_MAX_BOUNCES
+      && lw_plane_ground<HV_ALL>(S);
+}
+
+/* That transition; the event-part fields it sets are stored into slot s */
+__device__ __forceinline__ void
+transition(Path& p, const DScene& S, uint4* paths, uint32_t s, uint32_t P)
+{
+  if(p.state == ST_SW_SCAT_END) {
+    const float3 pn = sw_scat_volume(p, S);
+    paths[vec_at(s, kPnextV4, P)] =
+      make_uint4(__float_as_uint(pn.x), __float_as_uint(pn.y), __float_as_uint(pn.z), 0u);
+  } else {
+    float3 pos, dir;
+    lw_scatter_plane(p, S, pos, dir);
+    uint4* v = paths + vec_at(s, kPosV4, P);
+    ((uint2*)v)[1] = make_uint2(__float_as_uint(pos.x), __float_as_uint(pos.y));
+    v = paths + vec_at(s, kPosV4 + 1, P);
+    *v = make_uint4(__float_as_uint(pos.z), __float_as_uint(dir.x), __float_as_uint(dir.y),
+                    __float_as_uint(dir.z));
+  }
 }
 
 }  // namespace
@@ -237,15 +299,32 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
   p.state = ST_IDLE;
   bool have = false, drained = false;
   uint32_t s = 0, left = 0;
+#if HG_GAS_BATCH
+  uint32_t waited = 0; /* warp-uniform */
+#endif
+#if HG_FETCH_BATCH
+  uint32_t idle = 0; /* warp-uniform */
+#endif
   for(;;) {
     const bool need = !have && !drained;
-    const unsigned m = __ballot_sync(0xffffffffu, need);
+    unsigned m = __ballot_sync(0xffffffffu, need);
+#if HG_FETCH_BATCH
+    /* lanes whose path left wait until HG_FETCH_BATCH of them (or every
+     * lane) can load a new one, or for HG_FETCH_WAIT iterations: the warp
+     * then waits once on the loads of several paths */
+    if(m && __popc(m) < HG_FETCH_BATCH && __any_sync(0xffffffffu, have) && idle < HG_FETCH_WAIT) {
+      ++idle;
+      m = 0;
+    } else {
+      idle = 0;
+    }
+#endif
     if(m) {
       const unsigned leader = __ffs(m) - 1;
       uint32_t i0 = 0;
       if(lane == leader) i0 = atomicAdd(&ctl->fetch_trace, (uint32_t)__popc(m));
       i0 = __shfl_sync(0xffffffffu, i0, leader);
-      if(need) {
+      if(m & (1u << lane)) {
         const uint32_t idx = i0 + __popc(m & ((1u << lane) - 1u));
         if(idx < n) {
           s = list[idx];
@@ -259,25 +338,26 @@ k_wave_trace(WTables W, uint32_t b, int tables_in_smem)
       }
     }
     if(!__any_sync(0xffffffffu, have)) break;
-    if(have) {
-      trace_step<HV_ALL>(p, T.scenes[p.si]);
-      if(p.state == ST_SW_SCAT_END && p.tr.hit) {
-        /* a SW free path ended in the medium: its absorption trace runs
-         * here, without a round trip through the event stage */
-        const float3 pn = sw_scat_volume(p, T.scenes[p.si]);
-        W.paths[vec_at(s, kPnextV4, W.P)] =
-          make_uint4(__float_as_uint(pn.x), __float_as_uint(pn.y), __float_as_uint(pn.z), 0u);
-      } else if(p.state == ST_LW_END && p.tr.hit && p.tr.event == 1 && p.bounces < HG_MAX_BOUNCES
-             && lw_plane_ground<HV_ALL>(T.scenes[p.si])) {
-        /* a LW scattering in the medium: the walk goes on here */
-        float3 pos, dir;
-        lw_scatter_plane(p, T.scenes[p.si], pos, dir);
-        uint4* v = W.paths + vec_at(s, kPosV4, W.P);
-        ((uint2*)v)[1] = make_uint2(__float_as_uint(pos.x), __float_as_uint(pos.y));
-        v = W.paths + vec_at(s, kPosV4 + 1, W.P);
-        *v = make_uint4(__float_as_uint(pos.z), __float_as_uint(dir.x), __float_as_uint(dir.y),
-                        __float_as_uint(dir.z));
+    bool go = have;
+#if HG_GAS_BATCH
+    {
+      /* a gas region (an analytic column, several times a voxel step's code)
+       * waits until HG_GAS_BATCH lanes of the warp want one, or for
+       * HG_GAS_WAIT iterations, so that its code runs with more lanes */
+      const bool gas = have && trace_in_gas(p.tr);
+      const unsigned gm = __ballot_sync(0xffffffffu, gas);
+      const unsigned am = __ballot_sync(0xffffffffu, have);
+      if(gm && gm != am && __popc(gm) < HG_GAS_BATCH && waited < HG_GAS_WAIT) {
+        ++waited;
+        go = have && !gas;
+      } else {
+        waited = 0;
       }
+    }
+#endif
+    if(go) {
+      trace_step<HV_ALL>(p, T.scenes[p.si]);
+      if(transition_here(p, T.scenes[p.si])) transition(p, T.scenes[p.si], W.paths, s, W.P);
       if(p.state != ST_TRACE || --left == 0) {
         p.t0 = gtimer() - p.t0;
         store_trace(p, W.paths, s, W.P);
