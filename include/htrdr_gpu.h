@@ -352,9 +352,9 @@ htrdr_gpu_draw_maps_batched_accum_device(struct htrdr_gpu_batch_item* items, siz
                                          const struct htrdr_gpu_tuning* tuning,
                                          struct htrdr_gpu_stats* stats);
 HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
-/* Default tuning of a request mode: short LW paths want small blocks and
- * regrouping at every step, long SW/CIE walks larger blocks and sparser
- * regrouping. */
+/* Default tuning of a request mode: the wavefront engine (trace-stage blocks
+ * of 256, 256 voxel steps per visit, 2^20 path slots), its tail megakernel
+ * taking over below 25 000 live paths for SW, 100 000 for CIE and LW. */
 HTRDR_GPU_API void htrdr_gpu_mode_tuning(int mode, struct htrdr_gpu_tuning* tuning);
 /* Autotuner: times the candidate tunings (persistent: block size, queue
  * chunk, regroup period; wavefront: tail threshold, regroup period) on

@@ -52,8 +52,9 @@ main(int argc, char** argv)
 
   htrdr_gpu_default_tuning(&t);
   CHECK(t.block_size > 0 && t.block_size % 32 == 0 && t.queue_chunk >= 1);
-  htrdr_gpu_mode_tuning(HTRDR_GPU_FLUX_LW, &t);
   CHECK(t.engine == HTRDR_GPU_ENGINE_PERSISTENT);
+  htrdr_gpu_mode_tuning(HTRDR_GPU_FLUX_LW, &t);
+  CHECK(t.engine == HTRDR_GPU_ENGINE_WAVEFRONT && t.wave_tail > 0);
   htrdr_gpu_mode_tuning(HTRDR_GPU_IMAGE_CIE, &t);
   CHECK(t.engine == HTRDR_GPU_ENGINE_WAVEFRONT);
 

@@ -68,11 +68,12 @@ def test_engine_selection_and_mode_tuning_host_checks():
     cie = api.mode_tuning(S.MODE_IMAGE_CIE)
     for t in (lw, sw, cie):
         assert t.block_size % 32 == 0 and 0 < t.block_size <= 512 and t.queue_chunk >= 1
-    assert (lw.block_size, lw.regroup_period) != (sw.block_size, sw.regroup_period)
-    # short LW paths: the persistent megakernel; long SW/CIE walks: the wavefront
-    assert lw.engine == api.ENGINE_PERSISTENT
-    assert sw.engine == cie.engine == api.ENGINE_WAVEFRONT
-    assert sw.wave_tail > 0 and cie.wave_tail > 0
+    # every mode on the wavefront (LW walks run whole in its trace stage); the
+    # tail megakernel takes over earlier for LW and CIE than for SW
+    assert lw.engine == sw.engine == cie.engine == api.ENGINE_WAVEFRONT
+    assert sw.wave_tail > 0 and cie.wave_tail > 0 and lw.wave_tail > 0
+    assert lw.wave_tail == cie.wave_tail > sw.wave_tail
+    assert lw.trace_budget == sw.trace_budget == cie.trace_budget == 256
 
 
 def test_tuning_struct_and_engine_fields():
