@@ -102,7 +102,7 @@ def test_draw_map_engines_agree(gpu_lib):
     """htrdr_gpu_draw_map on the persistent engine (default, by-mode or given
     tuning) equals the plain engine, on host and device outputs."""
     import torch
-    lookups = 0
+    grid_bytes = 0
     for gs, req in _mix(gpu_lib):
         gs.set_engine(gpu_lib.ENGINE_PLAIN)
         plain, sp = gs.draw_map(req)
@@ -123,7 +123,7 @@ def test_draw_map_engines_agree(gpu_lib):
         # the same leaf-grid entries and majorant nodes
         assert sp["grid_bytes"] == spp["grid_bytes"] == sw["grid_bytes"]
         assert sp["nodes"] == spp["nodes"] == sw["nodes"]
-        lookups += sp["grid_bytes"]
+        grid_bytes += sp["grid_bytes"]
         t.trace_budget, t.wave_slots, t.wave_tail = 5, 333, 100
         gs.set_engine(gpu_lib.ENGINE_WAVEFRONT, t)
         wave2, _ = gs.draw_map(req)
@@ -134,7 +134,7 @@ def test_draw_map_engines_agree(gpu_lib):
         got = np.frombuffer(dev.cpu().numpy().tobytes(), dtype=pers.dtype).reshape(pers.shape)
         _cmp(got, plain, req.mode)
         gs.set_engine(gpu_lib.ENGINE_PERSISTENT)
-    assert lookups > 0
+    assert grid_bytes > 0
     gs, req = _mix(gpu_lib)[0]
     bad = gpu_lib.default_tuning()
     bad.block_size = 48  # not a multiple of a warp
