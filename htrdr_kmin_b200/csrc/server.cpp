@@ -367,7 +367,7 @@ htrdr_gpu_server::loop()
 bool
 htrdr_gpu_server::wave_setup()
 {
-  wave_P = cfg.tuning.wave_slots ? cfg.tuning.wave_slots : (1u << 20);
+  wave_P = cfg.tuning.wave_slots ? cfg.tuning.wave_slots : kDefaultWaveSlots;
   wave_tail = wave_serve_tail(cfg.tuning, cfg.device);
   const size_t rb = sizeof(Readback) + (kMaxReqs - 1) * sizeof(unsigned long long);
   bool ok = w_scenes.alloc(kMaxScenes * sizeof(DScene)) && w_reqs.alloc(kMaxReqs * sizeof(DRequest))

@@ -544,7 +544,7 @@ thread_wave(int device)
 static uint32_t
 wave_slots(const htrdr_gpu_tuning& tun, uint64_t total)
 {
-  uint64_t P = tun.wave_slots ? tun.wave_slots : (1u << 20);
+  uint64_t P = tun.wave_slots ? tun.wave_slots : kDefaultWaveSlots;
   if(P > total) P = total;
   if(P < 1) P = 1;
   return (uint32_t)P;

@@ -327,7 +327,7 @@ struct htrdr_gpu_tuning {
                            * the megakernel that finishes a wavefront run) */
   uint32_t blocks_per_sm; /* resident blocks per SM (0: occupancy maximum) */
   uint32_t engine;        /* HTRDR_GPU_ENGINE_PERSISTENT, _WAVEFRONT or _SORTED */
-  uint32_t wave_slots;    /* wavefront: paths in flight (0: 2^20, at most the realisations) */
+  uint32_t wave_slots;    /* wavefront: paths in flight (0: 2^21, at most the realisations) */
   uint32_t trace_budget;  /* wavefront: voxel steps of a trace per trace-stage visit (0: 256) */
   uint32_t wave_tail;     /* wavefront: live paths below which the remaining ones finish in one
                            * megakernel launch (0: four waves of its resident threads) */
@@ -353,7 +353,7 @@ htrdr_gpu_draw_maps_batched_accum_device(struct htrdr_gpu_batch_item* items, siz
                                          struct htrdr_gpu_stats* stats);
 HTRDR_GPU_API void htrdr_gpu_default_tuning(struct htrdr_gpu_tuning* tuning);
 /* Default tuning of a request mode: the wavefront engine (trace-stage blocks
- * of 256, 256 voxel steps per visit, 2^20 path slots), its tail megakernel
+ * of 256, 256 voxel steps per visit, 2^21 path slots), its tail megakernel
  * taking over below 25 000 live paths for SW, 100 000 for CIE and LW. */
 HTRDR_GPU_API void htrdr_gpu_mode_tuning(int mode, struct htrdr_gpu_tuning* tuning);
 /* Autotuner: times the candidate tunings (persistent: block size, queue
