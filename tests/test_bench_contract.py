@@ -83,3 +83,18 @@ def test_agreement_and_samples():
     a = bench.agreement(reqs, smp, cpu, gpu)
     assert a["n"] == 160 + 3 * 80 and a["pixels"] == 240
     assert a["frac_abs_z_gt_3"] < 0.03 and abs(a["mean_z"]) < 0.3
+
+
+def test_algorithmic_bytes_and_traffic_scaling():
+    """The roofline's byte model: 16 B per node fetch, the grid bytes the
+    device counted, 8 B per tentative collision, 32 B per realisation; the
+    recorded DRAM traffic of each engine scales with those bytes."""
+    import types
+    import bench
+    st = types.SimpleNamespace(nodes=3, grid_bytes=90, collisions=5, realisations=2)
+    assert bench.alg_bytes_of(st) == 16 * 3 + 90 + 8 * 5 + 32 * 2
+    for key in ("wavefront", "wavefront_lw"):
+        t1, src = bench.traffic_per_launch(key, 1000)
+        t2, _ = bench.traffic_per_launch(key, 2000)
+        assert src and t1 > 1000 and abs(t2 - 2 * t1) < 1e-6 * t2
+    assert bench.traffic_per_launch("no_such_kernel", 1000) == (None, None)
